@@ -1,0 +1,253 @@
+"""Python host binding of libbls_gpu.so (ctypes over the C ABI in include/bls_gpu.h).
+
+It mirrors the reference's Rust FFI crate (gpu-crypto/src/lib.rs,
+ic-integration/gpu_crypto/lib.rs): `init`, `batch_bls_verify`, `bls_verify`,
+`g1_decompress_batch`, with the same argument meaning and error behaviour
+(an error return from the library raises `GpuError`, the Rust crate's `Err`).
+`Context` wraps the extended API: device-resident public-key tables,
+compressed signatures with per-item decode status, and Miller / Gt values.
+
+There is no CPU path here.  If the shared library is missing or cannot load,
+every call raises; nothing falls back to a CPU implementation.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbls_gpu.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "bls_gpu.h")
+
+G2_COEFF_U64S = 68 * 36     # 2448, gpu-crypto/src/lib.rs:29
+G1_U64S = 12                # gpu-crypto/src/lib.rs:30
+
+BLS_OK = 0
+BLS_ERR_NODEV = -1
+BLS_ERR_INVALID = -2
+BLS_ERR_CUDA = -3
+BLS_ERR_NOMEM = -4
+BLS_ERR_TIMEOUT = -5
+BLS_ERR_FULL = -6
+
+BLS_ACCEPT = 1
+BLS_REJECT = 0
+ST_OK, ST_BAD_FLAGS, ST_X_NOT_CANONICAL, ST_NOT_ON_CURVE, ST_NOT_IN_SUBGROUP = 0, 1, 2, 3, 4
+SIG_AFFINE, SIG_COMPRESSED = 0, 1
+
+
+class GpuError(RuntimeError):
+    pass
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_batch", ctypes.c_int), ("max_pks", ctypes.c_int),
+                ("mem_cap_bytes", ctypes.c_size_t), ("threads_per_block", ctypes.c_int),
+                ("blocks_per_sm", ctypes.c_int)]
+
+
+class Batch(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("sig_format", ctypes.c_int), ("sigs", ctypes.c_void_p),
+                ("neg_hms", ctypes.c_void_p), ("pk_ids", ctypes.c_void_p),
+                ("miller_out", ctypes.c_void_p), ("gt_out", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libbls_gpu.so (raises if it is absent: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GpuError("libbls_gpu.so not built (run `make -C icp-gpu_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I = ctypes.c_void_p, ctypes.c_int
+        L.gpu_crypto_init.restype = I
+        L.gpu_batch_bls_verify.argtypes = [P, P, P, P, P, I]
+        L.gpu_batch_sha256.argtypes = [P, P, I, I]
+        L.gpu_g1_decompress_batch.argtypes = [P, P, I]
+        L.gpu_g1_decompress.argtypes = [P, P]
+        L.gpu_msm_g1.argtypes = [P, P, ctypes.c_size_t, P]
+        L.gpu_jacobian_to_affine.argtypes = [P, P]
+        L.bls_config_default.argtypes = [ctypes.POINTER(Config), I]
+        L.bls_config_default.restype = None
+        L.bls_ctx_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(P)]
+        L.bls_ctx_destroy.argtypes = [P]
+        L.bls_ctx_destroy.restype = None
+        L.bls_last_error.restype = ctypes.c_char_p
+        L.bls_pk_register_coeffs.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_int32)]
+        L.bls_pk_register_affine.argtypes = [P, P, ctypes.POINTER(ctypes.c_int32)]
+        L.bls_pk_table.argtypes = [P, ctypes.c_int32, P]
+        L.bls_verify_batch.argtypes = [P, ctypes.POINTER(Batch), P]
+        L.bls_verify_batch_device.argtypes = [P, ctypes.POINTER(Batch), P]
+        L.bls_ctx_sync.argtypes = [P]
+        L.bls_ctx_stream.argtypes = [P]
+        L.bls_ctx_stream.restype = P
+        L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
+        _lib = L
+    return _lib
+
+
+def last_error():
+    return lib().bls_last_error().decode()
+
+
+def _u64(a, shape_last=None):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    if shape_last is not None:
+        a = a.reshape(-1, shape_last)
+    return a
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+# ----------------------------------------------------------------------------
+# the reference crate's API (gpu-crypto/src/lib.rs)
+# ----------------------------------------------------------------------------
+
+def init():
+    """gpu-crypto/src/lib.rs:36-39: Ok when a CUDA device is present."""
+    if lib().gpu_crypto_init() != 0:
+        raise GpuError("No CUDA GPU found")
+
+
+def batch_bls_verify(sigs, neg_hm_points, g2_prepared, pk_prepared):
+    """gpu-crypto/src/lib.rs:82-125.  sigs, neg_hm_points: (M, 12) u64 affine
+    Montgomery; g2_prepared: (2448,) u64; pk_prepared: (M, 2448) u64.
+    Returns a list of M bools; raises GpuError when the kernel call fails."""
+    sigs = _u64(sigs, G1_U64S)
+    nhms = _u64(neg_hm_points, G1_U64S)
+    g2 = _u64(g2_prepared).reshape(-1)
+    pk = _u64(pk_prepared, G2_COEFF_U64S)
+    m = sigs.shape[0]
+    assert nhms.shape[0] == m and pk.shape[0] == m and g2.size == G2_COEFF_U64S
+    if m == 0:
+        return []
+    res = np.zeros(m, dtype=np.int32)
+    ret = lib().gpu_batch_bls_verify(_ptr(sigs), _ptr(nhms), _ptr(g2), _ptr(pk), _ptr(res), m)
+    if ret != 0:
+        raise GpuError("GPU kernel failed: " + last_error())
+    return [bool(r == 1) for r in res]
+
+
+def bls_verify(sig, neg_hm, g2_prepared, pk_prepared):
+    """gpu-crypto/src/lib.rs:129-148 without its CPU fallback: raises instead."""
+    return batch_bls_verify(_u64(sig, 12), _u64(neg_hm, 12), g2_prepared, _u64(pk_prepared, G2_COEFF_U64S))[0]
+
+
+def g1_decompress_batch(compressed_points):
+    """ic-integration/gpu_crypto/lib.rs:189-223: bytes of n x 48 -> (n, 12) u64."""
+    b = bytes(compressed_points)
+    if len(b) % 48 != 0:
+        raise GpuError("Input must be multiple of 48 bytes")
+    n = len(b) // 48
+    if n == 0:
+        return np.zeros((0, 12), dtype=np.uint64)
+    src = np.frombuffer(b, dtype=np.uint8)
+    out = np.zeros((n, 12), dtype=np.uint64)
+    if lib().gpu_g1_decompress_batch(_ptr(src), _ptr(out), n) != 0:
+        raise GpuError("GPU decompression failed: " + last_error())
+    return out
+
+
+# ----------------------------------------------------------------------------
+# extended API
+# ----------------------------------------------------------------------------
+
+class Context:
+    """A device context: stream, buffers and resident public-key tables."""
+
+    def __init__(self, device=0, max_batch=0, max_pks=0, mem_cap_bytes=0):
+        L = lib()
+        cfg = Config()
+        L.bls_config_default(ctypes.byref(cfg), device)
+        if max_batch:
+            cfg.max_batch = max_batch
+        if max_pks:
+            cfg.max_pks = max_pks
+        cfg.mem_cap_bytes = mem_cap_bytes
+        h = ctypes.c_void_p()
+        rc = L.bls_ctx_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != BLS_OK:
+            raise GpuError("bls_ctx_create failed (%d): %s" % (rc, last_error()))
+        self.h = h
+        self.lib = L
+
+    def close(self):
+        if self.h:
+            self.lib.bls_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != BLS_OK:
+            raise GpuError("%s failed (%d): %s" % (what, rc, last_error()))
+
+    def register_pk_coeffs(self, coeffs, is_identity=False):
+        c = _u64(coeffs).reshape(-1)
+        assert c.size == G2_COEFF_U64S
+        pid = ctypes.c_int32()
+        self._check(self.lib.bls_pk_register_coeffs(self.h, _ptr(c), int(is_identity), ctypes.byref(pid)),
+                    "bls_pk_register_coeffs")
+        return pid.value
+
+    def register_pk_affine(self, q24):
+        q = _u64(q24).reshape(-1)
+        assert q.size == 24
+        pid = ctypes.c_int32()
+        self._check(self.lib.bls_pk_register_affine(self.h, _ptr(q), ctypes.byref(pid)), "bls_pk_register_affine")
+        return pid.value
+
+    def pk_table(self, pk_id):
+        out = np.zeros(G2_COEFF_U64S, dtype=np.uint64)
+        self._check(self.lib.bls_pk_table(self.h, pk_id, _ptr(out)), "bls_pk_table")
+        return out
+
+    def verify(self, sigs, neg_hms, pk_ids, compressed=False, want_values=False):
+        """results (n,) int32: 1 accept, 0 reject, -status for a decode failure;
+        with want_values also the Miller-loop and Gt values, (n, 72) u64 each."""
+        nhms = _u64(neg_hms, 12)
+        n = nhms.shape[0]
+        if compressed:
+            s = np.ascontiguousarray(np.frombuffer(bytes(sigs), dtype=np.uint8) if not isinstance(sigs, np.ndarray)
+                                     else sigs, dtype=np.uint8).reshape(-1)
+            assert s.size == 48 * n
+        else:
+            s = _u64(sigs, 12)
+            assert s.shape[0] == n
+        ids = np.ascontiguousarray(pk_ids, dtype=np.int32).reshape(-1)
+        assert ids.size == n
+        res = np.zeros(n, dtype=np.int32)
+        ml = np.zeros((n, 72), dtype=np.uint64) if want_values else None
+        gt = np.zeros((n, 72), dtype=np.uint64) if want_values else None
+        b = Batch(n, SIG_COMPRESSED if compressed else SIG_AFFINE, _ptr(s), _ptr(nhms), _ptr(ids), _ptr(ml), _ptr(gt))
+        self._check(self.lib.bls_verify_batch(self.h, ctypes.byref(b), _ptr(res)), "bls_verify_batch")
+        return (res, ml, gt) if want_values else res
+
+    def verify_device(self, n, sigs_ptr, nhms_ptr, ids_ptr, res_ptr, compressed=False, ml_ptr=None, gt_ptr=None):
+        """Enqueue a verify on device-resident arrays (raw device pointers)."""
+        b = Batch(n, SIG_COMPRESSED if compressed else SIG_AFFINE, sigs_ptr, nhms_ptr, ids_ptr, ml_ptr, gt_ptr)
+        self._check(self.lib.bls_verify_batch_device(self.h, ctypes.byref(b), res_ptr), "bls_verify_batch_device")
+
+    def sync(self):
+        self._check(self.lib.bls_ctx_sync(self.h), "bls_ctx_sync")
+
+    def stream(self):
+        return self.lib.bls_ctx_stream(self.h)
+
+    def g1_decompress(self, compressed):
+        src = np.ascontiguousarray(np.frombuffer(bytes(compressed), dtype=np.uint8))
+        n = src.size // 48
+        xy = np.zeros((n, 12), dtype=np.uint64)
+        st = np.zeros(n, dtype=np.int32)
+        self._check(self.lib.bls_g1_decompress_status(self.h, _ptr(src), n, _ptr(xy), _ptr(st)),
+                    "bls_g1_decompress_status")
+        return st, xy

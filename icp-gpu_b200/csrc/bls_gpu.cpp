@@ -1,0 +1,469 @@
+// Host side of libbls_gpu.so: the reference's C ABI and the extended
+// context API declared in include/bls_gpu.h.
+//
+// Against the reference wrapper (gpu-crypto/cuda/api.cu:128-160), which does
+// five cudaMalloc / cudaFree pairs, synchronous copies and a device-wide
+// synchronise per call on the default stream, a context here owns one stream
+// and grow-only device and pinned-host buffers, so a steady stream of calls
+// allocates nothing; public-key line tables are registered once and stay on
+// the device.  Every entry point takes the context's mutex, so the library is
+// safe to call from many threads (the reference is not: its README's GPU_MUTEX
+// does not exist in its sources).
+#include "../../include/bls_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(BLS_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                        __FILE__, __LINE__);                                              \
+    } while (0)
+
+// G2 generator, affine Montgomery (x.c0, x.c1, y.c0, y.c1)
+const uint64_t kG2Gen[24] = {
+    0xf5f28fa202940a10ULL, 0xb3f5fb2687b4961aULL, 0xa1a893b53e2ae580ULL,
+    0x9894999d1a3caee9ULL, 0x6f67b7631863366bULL, 0x058191924350bcd7ULL,
+    0xa5a9c0759e23f606ULL, 0xaaa0c59dbccd60c3ULL, 0x3bb17e18e2867806ULL,
+    0x1b1ab6cc8541b367ULL, 0xc2b6ed0ef2158547ULL, 0x11922a097360edf3ULL,
+    0x4c730af860494c4aULL, 0x597cfa1f5e369c5aULL, 0xe7e6856caa0a635aULL,
+    0xbbefb5e96e0d495fULL, 0x07d3a975f0ef25a2ULL, 0x0083fd8e7e80dae5ULL,
+    0xadc0fc92df64b05dULL, 0x18aa270a2b1461dcULL, 0x86adac6a3be4eba0ULL,
+    0x79495c4ec93da33aULL, 0xe7175850a43ccaedULL, 0x0b2bc2a163de1bf2ULL};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct bls_ctx {
+    bls_config cfg{};
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    size_t dev_bytes = 0;  // bytes held on the device by this context
+
+    struct DevBuf {
+        void* p = nullptr;
+        size_t cap = 0;
+    };
+    struct HostBuf {
+        void* p = nullptr;
+        size_t cap = 0;
+    };
+    // per-call scratch
+    DevBuf d_sigs, d_nhms, d_pkidx, d_res, d_ml, d_gt, d_pk_items, d_g2_call, d_in, d_xy, d_st;
+    HostBuf h_sigs, h_nhms, h_pkidx, h_res;
+
+    // registered tables
+    uint64_t* d_g2 = nullptr;       // generator table
+    uint64_t* d_pk = nullptr;       // max_pks x 2448
+    uint8_t* d_pk_inf = nullptr;    // max_pks
+    int n_pks = 0;
+    std::vector<uint8_t> h_pk_inf;
+
+    int grow(DevBuf& b, size_t bytes) {
+        if (bytes <= b.cap) return BLS_OK;
+        size_t want = bytes + bytes / 4;
+        if (cfg.mem_cap_bytes && dev_bytes - b.cap + want > cfg.mem_cap_bytes) {
+            want = bytes;
+            if (dev_bytes - b.cap + want > cfg.mem_cap_bytes)
+                return fail(BLS_ERR_NOMEM, "device budget %zu bytes exceeded", cfg.mem_cap_bytes);
+        }
+        if (b.p) {
+            cudaFree(b.p);
+            dev_bytes -= b.cap;
+            b.p = nullptr;
+            b.cap = 0;
+        }
+        CK(cudaMalloc(&b.p, want));
+        b.cap = want;
+        dev_bytes += want;
+        return BLS_OK;
+    }
+    int grow(HostBuf& b, size_t bytes) {
+        if (bytes <= b.cap) return BLS_OK;
+        size_t want = bytes + bytes / 4;
+        if (b.p) cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        CK(cudaHostAlloc(&b.p, want, cudaHostAllocDefault));
+        b.cap = want;
+        return BLS_OK;
+    }
+    void release() {
+        for (DevBuf* b : {&d_sigs, &d_nhms, &d_pkidx, &d_res, &d_ml, &d_gt, &d_pk_items, &d_g2_call, &d_in,
+                          &d_xy, &d_st})
+            if (b->p) cudaFree(b->p);
+        for (HostBuf* b : {&h_sigs, &h_nhms, &h_pkidx, &h_res})
+            if (b->p) cudaFreeHost(b->p);
+        if (d_g2) cudaFree(d_g2);
+        if (d_pk) cudaFree(d_pk);
+        if (d_pk_inf) cudaFree(d_pk_inf);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int ctx_init(bls_ctx* c, const bls_config* cfg) {
+    c->cfg = *cfg;
+    if (c->cfg.max_batch <= 0) c->cfg.max_batch = 65536;
+    if (c->cfg.max_pks <= 0) c->cfg.max_pks = 1024;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(BLS_ERR_NODEV, "no CUDA device");
+    if (c->cfg.device < 0 || c->cfg.device >= count)
+        return fail(BLS_ERR_INVALID, "device %d out of range (%d devices)", c->cfg.device, count);
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    size_t pk_bytes = (size_t)c->cfg.max_pks * bls::kCoeffU64 * 8;
+    size_t need = pk_bytes + c->cfg.max_pks + bls::kCoeffU64 * 8 + 24 * 8;
+    if (c->cfg.mem_cap_bytes && need > c->cfg.mem_cap_bytes)
+        return fail(BLS_ERR_NOMEM, "pk tables (%zu bytes) exceed the device budget", need);
+    CK(cudaMalloc(&c->d_pk, pk_bytes));
+    CK(cudaMalloc(&c->d_pk_inf, c->cfg.max_pks));
+    CK(cudaMalloc(&c->d_g2, bls::kCoeffU64 * 8));
+    c->dev_bytes = pk_bytes + c->cfg.max_pks + bls::kCoeffU64 * 8;
+    c->h_pk_inf.assign(c->cfg.max_pks, 0);
+    CK(cudaMemsetAsync(c->d_pk_inf, 0, c->cfg.max_pks, c->stream));
+    // generator line table, computed on the device
+    uint64_t* d_q = nullptr;
+    CK(cudaMalloc(&d_q, sizeof kG2Gen));
+    CK(cudaMemcpyAsync(d_q, kG2Gen, sizeof kG2Gen, cudaMemcpyHostToDevice, c->stream));
+    CK(bls::launch_g2_prepare(d_q, 1, c->d_g2, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaFree(d_q));
+    return BLS_OK;
+}
+
+// default context behind the reference ABI (device 0, as the reference selects)
+std::mutex g_default_mu;
+bls_ctx* g_default = nullptr;
+
+int default_ctx(bls_ctx** out) {
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if (!g_default) {
+        auto* c = new bls_ctx();
+        bls_config cfg;
+        bls_config_default(&cfg, 0);
+        int rc = ctx_init(c, &cfg);
+        if (rc != BLS_OK) {
+            c->release();
+            delete c;
+            return rc;
+        }
+        g_default = c;
+    }
+    *out = g_default;
+    return BLS_OK;
+}
+
+int run_verify(bls_ctx* c, const bls::VerifyArgs& a) {
+    CK(bls::launch_verify(a, c->stream));
+    return BLS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void bls_config_default(bls_config* cfg, int device) {
+    memset(cfg, 0, sizeof *cfg);
+    cfg->device = device;
+    cfg->max_batch = 65536;
+    cfg->max_pks = 1024;
+}
+
+const char* bls_last_error(void) { return g_err.c_str(); }
+
+int bls_ctx_create(const bls_config* cfg, bls_ctx** out) {
+    if (!out) return fail(BLS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    bls_config def;
+    if (!cfg) {
+        bls_config_default(&def, 0);
+        cfg = &def;
+    }
+    auto* c = new bls_ctx();
+    int rc = ctx_init(c, cfg);
+    if (rc != BLS_OK) {
+        c->release();
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return BLS_OK;
+}
+
+void bls_ctx_destroy(bls_ctx* ctx) {
+    if (!ctx || ctx == g_default) return;
+    cudaSetDevice(ctx->cfg.device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->release();
+    delete ctx;
+}
+
+void* bls_ctx_stream(bls_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int bls_ctx_sync(bls_ctx* ctx) {
+    if (!ctx) return fail(BLS_ERR_INVALID, "ctx is NULL");
+    CK(cudaSetDevice(ctx->cfg.device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BLS_OK;
+}
+
+int bls_pk_register_coeffs(bls_ctx* ctx, const uint64_t* coeffs, int is_identity, int32_t* pk_id) {
+    if (!ctx || !coeffs || !pk_id) return fail(BLS_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (ctx->n_pks >= ctx->cfg.max_pks) return fail(BLS_ERR_FULL, "all %d pk slots used", ctx->cfg.max_pks);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int id = ctx->n_pks;
+    CK(cudaMemcpyAsync(ctx->d_pk + (size_t)id * bls::kCoeffU64, coeffs, bls::kCoeffU64 * 8,
+                       cudaMemcpyHostToDevice, ctx->stream));
+    uint8_t inf = is_identity ? 1 : 0;
+    ctx->h_pk_inf[id] = inf;
+    CK(cudaMemcpyAsync(ctx->d_pk_inf + id, &ctx->h_pk_inf[id], 1, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n_pks++;
+    *pk_id = id;
+    return BLS_OK;
+}
+
+int bls_pk_register_affine(bls_ctx* ctx, const uint64_t* q24, int32_t* pk_id) {
+    if (!ctx || !q24 || !pk_id) return fail(BLS_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (ctx->n_pks >= ctx->cfg.max_pks) return fail(BLS_ERR_FULL, "all %d pk slots used", ctx->cfg.max_pks);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int rc = ctx->grow(ctx->d_in, 24 * 8);
+    if (rc) return rc;
+    int id = ctx->n_pks;
+    CK(cudaMemcpyAsync(ctx->d_in.p, q24, 24 * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(bls::launch_g2_prepare((const uint64_t*)ctx->d_in.p, 1, ctx->d_pk + (size_t)id * bls::kCoeffU64,
+                              ctx->stream));
+    ctx->h_pk_inf[id] = 0;
+    CK(cudaMemcpyAsync(ctx->d_pk_inf + id, &ctx->h_pk_inf[id], 1, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n_pks++;
+    *pk_id = id;
+    return BLS_OK;
+}
+
+int bls_pk_table(bls_ctx* ctx, int32_t pk_id, uint64_t* coeffs) {
+    if (!ctx || !coeffs) return fail(BLS_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (pk_id < -1 || pk_id >= ctx->n_pks) return fail(BLS_ERR_INVALID, "unknown pk id %d", pk_id);
+    CK(cudaSetDevice(ctx->cfg.device));
+    const uint64_t* src = pk_id < 0 ? ctx->d_g2 : ctx->d_pk + (size_t)pk_id * bls::kCoeffU64;
+    CK(cudaMemcpyAsync(coeffs, src, bls::kCoeffU64 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BLS_OK;
+}
+
+int bls_verify_batch(bls_ctx* ctx, const bls_batch* b, int32_t* results) {
+    if (!ctx || !b || !results) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (b->n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (b->n == 0) return BLS_OK;
+    if (!b->sigs || !b->neg_hms || !b->pk_ids) return fail(BLS_ERR_INVALID, "NULL input array");
+    if (b->sig_format != BLS_SIG_AFFINE && b->sig_format != BLS_SIG_COMPRESSED)
+        return fail(BLS_ERR_INVALID, "unknown sig_format %d", b->sig_format);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (int i = 0; i < b->n; ++i)
+        if (b->pk_ids[i] < 0 || b->pk_ids[i] >= ctx->n_pks)
+            return fail(BLS_ERR_INVALID, "item %d: unknown pk id %d", i, b->pk_ids[i]);
+    CK(cudaSetDevice(ctx->cfg.device));
+    size_t n = (size_t)b->n;
+    size_t sig_bytes = n * (b->sig_format == BLS_SIG_COMPRESSED ? 48 : 96);
+    int rc;
+    if ((rc = ctx->grow(ctx->d_sigs, sig_bytes)) || (rc = ctx->grow(ctx->d_nhms, n * 96)) ||
+        (rc = ctx->grow(ctx->d_pkidx, n * 4)) || (rc = ctx->grow(ctx->d_res, n * 4)))
+        return rc;
+    if (b->miller_out && (rc = ctx->grow(ctx->d_ml, n * 576))) return rc;
+    if (b->gt_out && (rc = ctx->grow(ctx->d_gt, n * 576))) return rc;
+    if ((rc = ctx->grow(ctx->h_sigs, sig_bytes)) || (rc = ctx->grow(ctx->h_nhms, n * 96)) ||
+        (rc = ctx->grow(ctx->h_pkidx, n * 4)) || (rc = ctx->grow(ctx->h_res, n * 4)))
+        return rc;
+    memcpy(ctx->h_sigs.p, b->sigs, sig_bytes);
+    memcpy(ctx->h_nhms.p, b->neg_hms, n * 96);
+    memcpy(ctx->h_pkidx.p, b->pk_ids, n * 4);
+    CK(cudaMemcpyAsync(ctx->d_sigs.p, ctx->h_sigs.p, sig_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_nhms.p, ctx->h_nhms.p, n * 96, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_pkidx.p, ctx->h_pkidx.p, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    bls::VerifyArgs a{};
+    a.sigs = ctx->d_sigs.p;
+    a.sig_compressed = b->sig_format == BLS_SIG_COMPRESSED;
+    a.nhms = (const uint64_t*)ctx->d_nhms.p;
+    a.g2 = ctx->d_g2;
+    a.pk_tables = ctx->d_pk;
+    a.pk_index = (const int32_t*)ctx->d_pkidx.p;
+    a.pk_identity = ctx->d_pk_inf;
+    a.n = b->n;
+    a.results = (int32_t*)ctx->d_res.p;
+    a.ml_out = b->miller_out ? (uint64_t*)ctx->d_ml.p : nullptr;
+    a.gt_out = b->gt_out ? (uint64_t*)ctx->d_gt.p : nullptr;
+    if ((rc = run_verify(ctx, a))) return rc;
+    CK(cudaMemcpyAsync(ctx->h_res.p, a.results, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (b->miller_out) CK(cudaMemcpyAsync(b->miller_out, a.ml_out, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
+    if (b->gt_out) CK(cudaMemcpyAsync(b->gt_out, a.gt_out, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(results, ctx->h_res.p, n * 4);
+    return BLS_OK;
+}
+
+int bls_verify_batch_device(bls_ctx* ctx, const bls_batch* b, int32_t* results_device) {
+    if (!ctx || !b || !results_device) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (b->n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (b->n == 0) return BLS_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CK(cudaSetDevice(ctx->cfg.device));
+    bls::VerifyArgs a{};
+    a.sigs = b->sigs;
+    a.sig_compressed = b->sig_format == BLS_SIG_COMPRESSED;
+    a.nhms = b->neg_hms;
+    a.g2 = ctx->d_g2;
+    a.pk_tables = ctx->d_pk;
+    a.pk_index = b->pk_ids;
+    a.pk_identity = ctx->d_pk_inf;
+    a.n = b->n;
+    a.results = results_device;
+    a.ml_out = b->miller_out;
+    a.gt_out = b->gt_out;
+    return run_verify(ctx, a);
+}
+
+int bls_g1_decompress_status(bls_ctx* ctx, const uint8_t* in, int n, uint64_t* xy, int32_t* status) {
+    if (!ctx || !in || !xy || !status) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (n == 0) return BLS_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int rc;
+    if ((rc = ctx->grow(ctx->d_in, (size_t)n * 48)) || (rc = ctx->grow(ctx->d_xy, (size_t)n * 96)) ||
+        (rc = ctx->grow(ctx->d_st, (size_t)n * 4)))
+        return rc;
+    CK(cudaMemcpyAsync(ctx->d_in.p, in, (size_t)n * 48, cudaMemcpyHostToDevice, ctx->stream));
+    CK(bls::launch_g1_decompress((const uint8_t*)ctx->d_in.p, n, (uint64_t*)ctx->d_xy.p, (int32_t*)ctx->d_st.p,
+                                 ctx->stream));
+    CK(cudaMemcpyAsync(xy, ctx->d_xy.p, (size_t)n * 96, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(status, ctx->d_st.p, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BLS_OK;
+}
+
+// --------------------------------------------------------------- reference ABI
+
+int gpu_crypto_init(void) {
+    bls_ctx* c;
+    return default_ctx(&c) == BLS_OK ? 0 : -1;
+}
+
+int gpu_batch_bls_verify(const uint64_t* sigs, const uint64_t* neg_hms, const uint64_t* g2_coeffs,
+                         const uint64_t* pk_coeffs, int32_t* results, int M) {
+    if (M == 0) return 0;
+    if (M < 0 || !sigs || !neg_hms || !g2_coeffs || !pk_coeffs || !results) {
+        fail(BLS_ERR_INVALID, "invalid arguments");
+        return -1;
+    }
+    bls_ctx* c;
+    if (default_ctx(&c) != BLS_OK) return -1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto body = [&]() -> int {
+        CK(cudaSetDevice(c->cfg.device));
+        size_t n = (size_t)M;
+        int rc;
+        if ((rc = c->grow(c->d_sigs, n * 96)) || (rc = c->grow(c->d_nhms, n * 96)) ||
+            (rc = c->grow(c->d_pk_items, n * bls::kCoeffU64 * 8)) || (rc = c->grow(c->d_g2_call, bls::kCoeffU64 * 8)) ||
+            (rc = c->grow(c->d_res, n * 4)))
+            return rc;
+        CK(cudaMemcpyAsync(c->d_sigs.p, sigs, n * 96, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->d_nhms.p, neg_hms, n * 96, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->d_g2_call.p, g2_coeffs, bls::kCoeffU64 * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->d_pk_items.p, pk_coeffs, n * bls::kCoeffU64 * 8, cudaMemcpyHostToDevice, c->stream));
+        bls::VerifyArgs a{};
+        a.sigs = c->d_sigs.p;
+        a.sig_compressed = 0;
+        a.nhms = (const uint64_t*)c->d_nhms.p;
+        a.g2 = (const uint64_t*)c->d_g2_call.p;
+        a.pk_tables = (const uint64_t*)c->d_pk_items.p;
+        a.pk_index = nullptr;
+        a.pk_identity = nullptr;
+        a.n = M;
+        a.results = (int32_t*)c->d_res.p;
+        if ((rc = run_verify(c, a))) return rc;
+        CK(cudaMemcpyAsync(results, a.results, n * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return BLS_OK;
+    };
+    return body() == BLS_OK ? 0 : -1;
+}
+
+int gpu_batch_sha256(const uint8_t*, uint8_t*, int, int) {
+    fail(BLS_ERR_INVALID, "gpu_batch_sha256 is not provided by this library");
+    return -1;
+}
+
+int gpu_g1_decompress_batch(const unsigned char* compressed, unsigned char* out_points, int n) {
+    if (n <= 0 || !compressed || !out_points) {
+        fail(BLS_ERR_INVALID, "invalid arguments");
+        return -1;
+    }
+    bls_ctx* c;
+    if (default_ctx(&c) != BLS_OK) return -1;
+    std::vector<int32_t> st((size_t)n);
+    std::vector<uint64_t> xy((size_t)n * 12);
+    if (bls_g1_decompress_status(c, compressed, n, xy.data(), st.data()) != BLS_OK) return -1;
+    for (int i = 0; i < n; ++i) {
+        if (st[i] != BLS_ST_OK) {
+            fail(BLS_ERR_INVALID, "point %d: decode status %d", i, st[i]);
+            return -1;
+        }
+        bool x0 = true;
+        for (int k = 0; k < 6; ++k) x0 = x0 && xy[12 * (size_t)i + k] == 0;
+        if (x0) {
+            fail(BLS_ERR_INVALID, "point %d is the identity", i);
+            return -1;
+        }
+    }
+    memcpy(out_points, xy.data(), (size_t)n * 96);
+    return 0;
+}
+
+int gpu_g1_decompress(const unsigned char* compressed, unsigned char* out_point) {
+    return gpu_g1_decompress_batch(compressed, out_point, 1);
+}
+
+int gpu_msm_g1(const uint8_t*, const uint8_t*, size_t, uint8_t*) {
+    fail(BLS_ERR_INVALID, "gpu_msm_g1 is not provided by this library");
+    return -1;
+}
+
+int gpu_jacobian_to_affine(const uint8_t*, uint8_t*) {
+    fail(BLS_ERR_INVALID, "gpu_jacobian_to_affine is not provided by this library");
+    return -1;
+}
+
+}  // extern "C"

@@ -1,0 +1,29 @@
+// Internal interface between the host library (bls_gpu.cpp) and the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bls {
+
+constexpr int kVerifyThreads = 64;
+constexpr int kCoeffU64 = 2448;
+
+struct VerifyArgs {
+    const void* sigs;            // n x 12 u64 (affine) or n x 48 B (compressed), device
+    int sig_compressed;
+    const uint64_t* nhms;        // n x 12 u64, device
+    const uint64_t* g2;          // generator line table, device
+    const uint64_t* pk_tables;   // k x 2448 u64, device
+    const int32_t* pk_index;     // n table ids, device; NULL = table i for item i
+    const uint8_t* pk_identity;  // per table, device; NULL = none is the identity
+    int n;
+    int32_t* results;            // n, device
+    uint64_t* ml_out;            // n x 72 or NULL, device
+    uint64_t* gt_out;            // n x 72 or NULL, device
+};
+
+cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
+cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
+cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStream_t s);
+
+}  // namespace bls

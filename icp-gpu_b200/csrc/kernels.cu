@@ -1,0 +1,89 @@
+// Device kernels of the verify path and their launchers.
+//
+//   k_verify          one verification per thread: optional G1 decode of the
+//                     signature, two-pair Miller loop, final exponentiation,
+//                     identity test (gpu-crypto/cuda/api.cu:80-109).  The
+//                     generator's line table is read by every thread at the same
+//                     address (broadcast); public-key tables are read per item.
+//   k_g1_decompress   one 48-byte point per thread (cuda/decompress.cu:140-188)
+//                     plus the from_compressed checks.
+//   k_g2_prepare      one G2 line table per thread (cuda/test_miller_v2.cu:148-229).
+#include <cuda_runtime.h>
+
+#include "g1.cuh"
+#include "g2prep.cuh"
+#include "internal.h"
+
+namespace bls {
+
+__global__ void __launch_bounds__(kVerifyThreads) k_verify(VerifyArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    fp sx, sy;
+    bool sig_id;
+    if (a.sig_compressed) {
+        int32_t st = g1_decode((const uint8_t*)a.sigs + 48 * (size_t)i, sx, sy, sig_id, true);
+        if (st != ST_OK) {
+            a.results[i] = -st;
+            if (a.ml_out) for (int k = 0; k < 72; ++k) a.ml_out[72 * (size_t)i + k] = 0;
+            if (a.gt_out) for (int k = 0; k < 72; ++k) a.gt_out[72 * (size_t)i + k] = 0;
+            return;
+        }
+    } else {
+        const uint64_t* s = (const uint64_t*)a.sigs + 12 * (size_t)i;
+        sx = fp_load_u64(s);
+        sy = fp_load_u64(s + 6);
+        sig_id = g1_limbs_identity(sx, sy);
+    }
+    const uint64_t* h = a.nhms + 12 * (size_t)i;
+    fp hx = fp_load_u64(h), hy = fp_load_u64(h + 6);
+    bool h_id = g1_limbs_identity(hx, hy);
+    int64_t pk = a.pk_index ? (int64_t)a.pk_index[i] : (int64_t)i;
+    bool pk_id = a.pk_identity ? a.pk_identity[pk] != 0 : false;
+    fp12 ml = miller_loop_2(sx, sy, a.g2, sig_id, hx, hy, a.pk_tables + BLS_COEFF_U64 * pk, h_id || pk_id);
+    fp12 gt = final_exponentiation(ml);
+    a.results[i] = fp12_is_one(gt) ? 1 : 0;
+    if (a.ml_out) fp12_store_u64(a.ml_out + 72 * (size_t)i, ml);
+    if (a.gt_out) fp12_store_u64(a.gt_out + 72 * (size_t)i, gt);
+}
+
+__global__ void __launch_bounds__(128) k_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    fp x, y;
+    bool id;
+    int32_t st = g1_decode(in + 48 * (size_t)i, x, y, id, true);
+    status[i] = st;
+    fp_store_u64(xy + 12 * (size_t)i, x);
+    fp_store_u64(xy + 12 * (size_t)i + 6, y);
+}
+
+__global__ void __launch_bounds__(64) k_g2_prepare(const uint64_t* q, int n, uint64_t* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t* qi = q + 24 * (size_t)i;
+    fp2 qx = {fp_load_u64(qi), fp_load_u64(qi + 6)};
+    fp2 qy = {fp_load_u64(qi + 12), fp_load_u64(qi + 18)};
+    g2_prepare(qx, qy, out + BLS_COEFF_U64 * (size_t)i);
+}
+
+cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s) {
+    if (a.n <= 0) return cudaSuccess;
+    int blocks = (a.n + kVerifyThreads - 1) / kVerifyThreads;
+    k_verify<<<blocks, kVerifyThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_g1_decompress<<<(n + 127) / 128, 128, 0, s>>>(in, n, xy, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_g2_prepare<<<(n + 63) / 64, 64, 0, s>>>(q, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace bls

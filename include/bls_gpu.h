@@ -1,0 +1,166 @@
+/*
+ * libbls_gpu.so - BLS12-381 batch signature verification on NVIDIA B200 (sm_100a).
+ *
+ * Part 1 is the reference's C ABI, symbol for symbol, so the reference's Rust
+ * FFI crates link or dlopen this library unchanged.  Part 2 is the extended
+ * API: device-resident public-key line tables, compressed signatures with
+ * per-item decode status, Miller-loop / Gt values for parity checks, batched
+ * persistent launches and a serving loop.
+ *
+ * Data formats (same as the reference):
+ *   Fp      6 x uint64 little-endian limbs of a*R mod p, R = 2^384 (the
+ *           in-memory form of ic_bls12_381's Fp), always < p.
+ *   G1      12 x uint64: x[6], y[6] affine, Montgomery.  The identity is
+ *           x = 0 with y = 0 or y = R mod p (no curve point has x = 0); a pair
+ *           holding an identity contributes nothing to the Miller loop, as in
+ *           ic_bls12_381's multi_miller_loop.
+ *   G2 line table  2448 x uint64: ic_bls12_381 G2Prepared coefficients,
+ *           68 x (c0, c1, c2), each an Fp2 (c0[6], c1[6]).
+ *   Gt / Miller values  72 x uint64: 12 Fp in tower order
+ *           c0.c0.c0, c0.c0.c1, c0.c1.c0, ..., c1.c2.c1.
+ *   Compressed G1  48 bytes, ZCash BLS12-381 encoding (big-endian x, flags
+ *           0x80 compressed, 0x40 infinity, 0x20 y lexicographically largest).
+ *
+ * All pointers are host memory owned by the caller unless a name says
+ * "device".  Every entry point is thread-safe.
+ */
+#ifndef BLS_GPU_H
+#define BLS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================
+ * Part 1: the reference ABI
+ * ==================================================================== */
+
+/* Replaces gpu_crypto_init, gpu-crypto/cuda/api.cu:118-124.
+ * 0 when a CUDA device is present (device 0 is selected), -1 otherwise. */
+int gpu_crypto_init(void);
+
+/* Replaces gpu_batch_bls_verify, gpu-crypto/cuda/api.cu:128-160
+ * (Rust binding gpu-crypto/src/lib.rs:18-25).
+ * results[i] = 1 when e(sigs[i], G2) * e(neg_hms[i], pk_i) == 1, else 0, where
+ * pk_i's line table is pk_coeffs + 2448*i and g2_coeffs is the generator's.
+ * M == 0 returns 0; M < 0, a NULL pointer or a CUDA error returns -1. */
+int gpu_batch_bls_verify(const uint64_t* sigs, const uint64_t* neg_hms, const uint64_t* g2_coeffs,
+                         const uint64_t* pk_coeffs, int32_t* results, int M);
+
+/* Replaces gpu_batch_sha256, gpu-crypto/cuda/api.cu:165-186.  SHA-256 is not
+ * on the verify path this library implements: always returns -1, which the
+ * reference's callers treat as "use the CPU". */
+int gpu_batch_sha256(const uint8_t* chunks, uint8_t* hashes, int N, int chunk_size);
+
+/* Replaces gpu_g1_decompress_batch, cuda/decompress.cu:198-226 (dlopen'd by
+ * ic-integration/gpu_crypto/lib.rs:92-122).  out: n x 96 bytes, Montgomery x
+ * then y.  Unlike the reference, every point is validated exactly as
+ * G1Affine::from_compressed does; 0 when all n points decode to non-identity
+ * points, -1 when n <= 0, a pointer is NULL, any point is invalid or is the
+ * identity (the 96-byte output cannot carry the infinity flag, so the caller
+ * falls back to its CPU decoder, which reports the precise error), or on a
+ * CUDA error.  Per-item reasons: bls_g1_decompress_status. */
+int gpu_g1_decompress_batch(const unsigned char* compressed, unsigned char* out_points, int n);
+
+/* Replaces gpu_g1_decompress, cuda/decompress.cu:229-231 (n = 1). */
+int gpu_g1_decompress(const unsigned char* compressed, unsigned char* out_point);
+
+/* Replace gpu_msm_g1 / gpu_jacobian_to_affine (ic-integration/gpu_crypto/cuda/
+ * msm.cu:32; resolved together at ic-integration/gpu_crypto/lib.rs:103-107).
+ * Multi-scalar multiplication is not on the verify path: both return -1 so
+ * the caller keeps its CPU MSM.  They exist so the dlopen symbol check passes. */
+int gpu_msm_g1(const uint8_t* points, const uint8_t* scalars, size_t n, uint8_t* result_jacobian);
+int gpu_jacobian_to_affine(const uint8_t* jacobian, uint8_t* affine);
+
+/* ======================================================================
+ * Part 2: extended API (no counterpart in the reference; it extends the
+ * reference's verify path above)
+ * ==================================================================== */
+
+/* return codes */
+#define BLS_OK 0
+#define BLS_ERR_NODEV (-1)
+#define BLS_ERR_INVALID (-2)
+#define BLS_ERR_CUDA (-3)
+#define BLS_ERR_NOMEM (-4)
+#define BLS_ERR_TIMEOUT (-5)
+#define BLS_ERR_FULL (-6)
+
+/* per-item results of the extended verify calls */
+#define BLS_ACCEPT 1
+#define BLS_REJECT 0
+/* decode failures are reported as the negated status below */
+#define BLS_ST_OK 0
+#define BLS_ST_BAD_FLAGS 1         /* compression bit clear, or infinity with payload / sort bit */
+#define BLS_ST_X_NOT_CANONICAL 2   /* x >= p */
+#define BLS_ST_NOT_ON_CURVE 3      /* x^3 + 4 is not a square */
+#define BLS_ST_NOT_IN_SUBGROUP 4   /* on the curve, outside the order-r subgroup */
+
+/* signature input formats */
+#define BLS_SIG_AFFINE 0      /* 12 x uint64 Montgomery x, y */
+#define BLS_SIG_COMPRESSED 1  /* 48-byte ZCash encoding, decoded and validated on the GPU */
+
+typedef struct bls_ctx bls_ctx;
+
+typedef struct {
+    int device;             /* CUDA device ordinal */
+    int max_batch;          /* items per launch preallocated (grown on demand; 0 = 65536) */
+    int max_pks;            /* public-key table slots (0 = 1024) */
+    size_t mem_cap_bytes;   /* device-memory budget for this context (0 = none) */
+    int threads_per_block;  /* 0 = library default */
+    int blocks_per_sm;      /* persistent launches: 0 = occupancy maximum */
+} bls_config;
+
+typedef struct {
+    int n;                     /* items */
+    int sig_format;            /* BLS_SIG_AFFINE or BLS_SIG_COMPRESSED */
+    const void* sigs;          /* n x 12 uint64, or n x 48 bytes */
+    const uint64_t* neg_hms;   /* n x 12 uint64: -H(m_i), affine Montgomery */
+    const int32_t* pk_ids;     /* n ids from bls_pk_register_* */
+    uint64_t* miller_out;      /* optional n x 72: Miller-loop value (NULL = skip) */
+    uint64_t* gt_out;          /* optional n x 72: final exponentiation (NULL = skip) */
+} bls_batch;
+
+/* fill *cfg with defaults for `device` */
+void bls_config_default(bls_config* cfg, int device);
+
+/* create / destroy a context: its own stream, device buffers, pk tables */
+int bls_ctx_create(const bls_config* cfg, bls_ctx** out);
+void bls_ctx_destroy(bls_ctx* ctx);
+
+/* last error message of the calling thread ("" when none) */
+const char* bls_last_error(void);
+
+/* Register a public key; its line table stays on the device for the life of
+ * the context.  From a caller-computed table (reference layout): */
+int bls_pk_register_coeffs(bls_ctx* ctx, const uint64_t* coeffs2448, int is_identity, int32_t* pk_id);
+/* From an affine point (x.c0, x.c1, y.c0, y.c1: 24 x uint64 Montgomery); the
+ * line table is computed on the GPU.  The caller vouches that the point is in G2. */
+int bls_pk_register_affine(bls_ctx* ctx, const uint64_t* q24, int32_t* pk_id);
+/* copy a registered table back (tests) */
+int bls_pk_table(bls_ctx* ctx, int32_t pk_id, uint64_t* coeffs2448);
+
+/* Verify one batch, synchronously.  results[i] = BLS_ACCEPT, BLS_REJECT or
+ * -(decode status) for a compressed signature that fails to decode. */
+int bls_verify_batch(bls_ctx* ctx, const bls_batch* batch, int32_t* results);
+
+/* Same with every pointer in device memory (inputs already resident); the
+ * call enqueues on the context stream and returns without synchronising.
+ * bls_ctx_sync waits for it. */
+int bls_verify_batch_device(bls_ctx* ctx, const bls_batch* batch_device, int32_t* results_device);
+int bls_ctx_sync(bls_ctx* ctx);
+/* the context's CUDA stream (cudaStream_t) */
+void* bls_ctx_stream(bls_ctx* ctx);
+
+/* Decode n compressed G1 points: status[i] (BLS_ST_*), xy[i] 12 x uint64
+ * (identity: x = 0, y = R mod p; failures: zeros). */
+int bls_g1_decompress_status(bls_ctx* ctx, const uint8_t* compressed, int n, uint64_t* xy, int32_t* status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLS_GPU_H */
