@@ -1,0 +1,345 @@
+"""BLS12-381 batch verification bench (one JSON line on rank 0).
+
+Workload (the headline configuration): 4,096 verifications against 40
+distinct public keys whose G2 line tables are computed once on the device and
+kept resident; 1 in 8 items corrupted (half message flip, half wrong key), so
+the expected accept bits are known and checked after timing.
+
+  value  verifies/s with inputs resident in HBM: one verify launch per step,
+         timed with CUDA events on the library's stream; L2 flushed (256 MiB
+         write) between steps, outside the timed interval.
+  e2e    verifies/s through the C ABI call (bls_verify_batch) from host
+         buffers: host->device copies, kernel, result copy-back per step.
+  roofline  INT32 IMAD pipe: counted IMAD-pipe instructions per verify
+         (Fp multiplies of this implementation x 588) / kernel time, against
+         SMs x 64 IMAD/clk x the SM clock sampled during the timed region.
+  cpu_baseline  the oracle (C++ restatement of the reference CPU verifier)
+         on all host cores, bounded sample of the same workload.
+
+--impl reference runs the reference's CPU verifier (the oracle port; the
+reference's Rust crates cannot be built here) on the same workload.
+Multi-GPU (torchrun): every rank verifies its own 4,096 items (weak scaling);
+the step time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "icp-gpu_b200"))
+
+import numpy as np  # noqa: E402
+
+N_ITEMS = 4096
+N_KEYS = 40
+SEED = 2
+METRIC = "BLS12-381 verifies/s, batched vs plain launch, bit-exact; serve p50/p99 ms"
+
+# Fp multiplies per verification in this implementation (icp-gpu_b200/csrc):
+#   Miller loop: 136 line evaluations x 43 (mul_by_014 39 + 2 x fp2_mul_fp 2)
+#                + 62 Fp12 squarings x 36                         = 8,080
+#   final exp:   easy part 861 (inverse 719, 2 Fp12 mul, Frobenius^2)
+#                + 2 cyclotomic squares x 18 + 5 cyc_exp x 1,404
+#                + 10 Fp12 mul x 54 + 6 Frobenius x 17            = 8,559
+# and 588 IMAD-pipe instructions per multiply (12 rows x (48 mad + 1 mul.lo)).
+FP_MULS_PER_VERIFY = 8080 + 8559
+IMAD_PER_FP_MUL = 588
+IMAD_PER_VERIFY = FP_MULS_PER_VERIFY * IMAD_PER_FP_MUL
+IMAD_PER_CLK_PER_SM = 64
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons, samples = [], None, set(), 0
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            samples += 1
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": samples}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------- CPU (oracle) legs
+
+def cpu_verifier():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cpu as C  # the checker / reference CPU verifier restated (oracle/)
+    return C
+
+
+def cpu_rate(C, wl, g2, count, threads):
+    t = time.perf_counter()
+    r = C.verify_batch(wl["sigs"][:count], wl["nhms"][:count], g2, wl["pk_tables"],
+                       pk_index=wl["pk_index"][:count], nthreads=threads)
+    dt = time.perf_counter() - t
+    assert (r == wl["expect"][:count]).all(), "CPU verifier disagrees with the expected accept bits"
+    return count / dt, dt
+
+
+def cpu_baseline(wl, g2, target_s=12.0):
+    C = cpu_verifier()
+    threads = C.num_threads()
+    calib = min(N_ITEMS, max(64, 4 * threads))
+    rate, dt = cpu_rate(C, wl, g2, calib, threads)
+    count = int(min(N_ITEMS, max(calib, rate * target_s)))
+    rate, dt = cpu_rate(C, wl, g2, count, threads)
+    return {"value": rate, "unit": "verifies/s", "cores": threads, "kind": "port",
+            "sample": "%d of the %d workload items, oracle/cpu_verifier.cpp on %d host threads, %.1f s"
+                      % (count, N_ITEMS, threads, dt)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import workload as WL
+    wl = WL.config_keyset(N_ITEMS, N_KEYS, seed=SEED)
+    g2 = generator_table(WL)
+    C = cpu_verifier()
+    threads = C.num_threads()
+    rate, _ = cpu_rate(C, wl, g2, min(N_ITEMS, max(64, 4 * threads)), threads)
+    per_step = int(min(N_ITEMS, max(threads, rate * 4.0)))  # about 4 s of CPU work per step
+    for _ in range(args.warmup):
+        cpu_rate(C, wl, g2, min(per_step, threads), threads)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_rate(C, wl, g2, per_step, threads)
+        times.append(dt)
+    total = sum(times)
+    value = per_step * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "verifies/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "keyset-4096-40: 4,096 verifications over 40 public keys (configs[1])",
+                   "step_sample": per_step, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "verifies/s", "cores": threads, "kind": "port",
+                         "sample": "%d items per step of the 4,096-item workload" % per_step},
+        "e2e": {"value": value, "unit": "verifies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU verifier = oracle/cpu_verifier.cpp (restatement of ic_bls12_381's verify as the "
+                "reference's GPU code mirrors it); the reference's Rust crates are not buildable offline",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def generator_table(WL):
+    g = np.array([[0xf5f28fa202940a10, 0xb3f5fb2687b4961a, 0xa1a893b53e2ae580, 0x9894999d1a3caee9,
+                   0x6f67b7631863366b, 0x058191924350bcd7, 0xa5a9c0759e23f606, 0xaaa0c59dbccd60c3,
+                   0x3bb17e18e2867806, 0x1b1ab6cc8541b367, 0xc2b6ed0ef2158547, 0x11922a097360edf3,
+                   0x4c730af860494c4a, 0x597cfa1f5e369c5a, 0xe7e6856caa0a635a, 0xbbefb5e96e0d495f,
+                   0x07d3a975f0ef25a2, 0x0083fd8e7e80dae5, 0xadc0fc92df64b05d, 0x18aa270a2b1461dc,
+                   0x86adac6a3be4eba0, 0x79495c4ec93da33a, 0xe7175850a43ccaed, 0x0b2bc2a163de1bf2]],
+                 dtype=np.uint64)
+    return WL.g2_prepare(g)[0]
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def run_gpu(args):
+    import torch
+    import bls_gpu as G
+    import workload as WL
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    wl = WL.config_keyset(N_ITEMS, N_KEYS, seed=SEED + rank)
+    ctx = G.Context(device=local)
+    ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
+    for i in (0, N_KEYS - 1):  # device tables == caller-built tables
+        assert (ctx.pk_table(int(ids[i])) == wl["pk_tables"][i]).all()
+    pk_ids = ids[wl["pk_index"]]
+
+    dev = torch.device("cuda", local)
+    d_sigs = torch.from_numpy(wl["sigs"].view(np.int64)).to(dev)
+    d_nhms = torch.from_numpy(wl["nhms"].view(np.int64)).to(dev)
+    d_ids = torch.from_numpy(pk_ids).to(dev)
+    d_res = torch.zeros(N_ITEMS, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        ctx.verify_device(N_ITEMS, d_sigs.data_ptr(), d_nhms.data_ptr(), d_ids.data_ptr(), d_res.data_ptr())
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+    ctx.sync()
+    res = d_res.cpu().numpy()
+    assert (res == wl["expect"]).all(), "GPU accept bits differ from the expected ones"
+
+    props = torch.cuda.get_device_properties(dev)
+    sms = props.multi_processor_count
+    sampler = ClockSampler(local)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if pg:
+        pg.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if pg:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    res = d_res.cpu().numpy()
+    assert (res == wl["expect"]).all(), "GPU accept bits differ from the expected ones (timed run)"
+    value = N_ITEMS * world * args.steps / (total_ms / 1e3)
+    kernel_ms = statistics.mean(step_ms)
+
+    # e2e through the C ABI from host buffers
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ctx.sync()
+        t0 = time.perf_counter()
+        r = ctx.verify(wl["sigs"], wl["nhms"], pk_ids)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            e2e_times.append(dt)
+    assert (r == wl["expect"]).all()
+    e2e_s = sum(e2e_times)
+    if pg:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = N_ITEMS * world * args.steps / e2e_s
+
+    result = None
+    if rank == 0:
+        clk = clocks["sm_mhz"] or float(load_peaks().get("sm_max_mhz", 1965.0))
+        peak_timad = sms * IMAD_PER_CLK_PER_SM * clk * 1e6 / 1e12
+        achieved_timad = IMAD_PER_VERIFY * N_ITEMS / (kernel_ms / 1e3) / 1e12
+        roofline = {
+            "bound": "int32-imad", "achieved": round(achieved_timad, 3), "peak": round(peak_timad, 3),
+            "unit": "TIMAD/s", "frac": round(achieved_timad / peak_timad, 4), "traffic": None,
+            "peak_basis": "%d SMs x 64 IMAD/clk x %.0f MHz (median SM clock sampled during the timed region)"
+                          % (sms, clk),
+            "imad_per_verify": IMAD_PER_VERIFY, "fp_muls_per_verify": FP_MULS_PER_VERIFY,
+            "kernel": "k_verify", "kernel_ms": round(kernel_ms, 4),
+        }
+        result = {
+            "metric": METRIC, "value": round(value, 1), "unit": "verifies/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded keys, RFC 9380 hash-to-G1, signatures; 1 in 8 corrupted)",
+            "config": {"workload": "keyset-4096-40: 4,096 verifications over 40 device-resident public keys "
+                                   "(configs[1])", "items_per_gpu": N_ITEMS, "keys": N_KEYS,
+                       "parallelism": "replicas: independent shards per GPU, no collective",
+                       "l2": "flushed between steps (256 MiB write), outside the timed interval"},
+            "e2e": {"value": round(e2e_value, 1), "unit": "verifies/s",
+                    "h2d_bytes_per_step": int(wl["sigs"].nbytes + wl["nhms"].nbytes + pk_ids.nbytes),
+                    "d2h_bytes_per_step": int(N_ITEMS * 4), "api": "bls_verify_batch (C ABI, host buffers)"},
+            "roofline": roofline,
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+            "bit_exact": True,
+        }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(wl, generator_table(WL))
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -193,3 +193,57 @@ def test_hash_to_g1_in_subgroup():
         h = B.hash_to_g1(m, W.DST)
         assert B.g1_on_curve(h) and B.g1_in_subgroup(h)
     assert B.hash_to_g1(b"abc", W.DST) != B.hash_to_g1(b"abd", W.DST)
+
+
+# ---------------------------------------------------------------- workload generator vs oracle
+
+def test_generator_sha256_and_xmd():
+    import hashlib
+    import workload as WL
+    L = WL.wl()
+    for m in (b"", b"abc", bytes(range(200))):
+        o = np.zeros(32, np.uint8)
+        a = np.frombuffer(m, np.uint8) if m else np.zeros(1, np.uint8)
+        L.wl_sha256(a.ctypes.data, len(m), o.ctypes.data)
+        assert bytes(o) == hashlib.sha256(m).digest()
+    o = np.zeros(128, np.uint8)
+    m = np.frombuffer(b"abc", np.uint8)
+    d = np.frombuffer(W.DST, np.uint8)
+    L.wl_expand_message_xmd(m.ctypes.data, 3, d.ctypes.data, len(W.DST), o.ctypes.data, 128)
+    assert bytes(o) == B.expand_message_xmd(b"abc", W.DST, 128)
+
+
+def test_generator_hash_sign_keys_match_oracle():
+    import workload as WL
+    msgs = [bytes([i]) * 32 for i in range(4)]
+    h = WL.hash_to_g1(msgs)
+    for i, m in enumerate(msgs):
+        assert list(h[i]) == B.g1_to_mont_u64(B.hash_to_g1(m, W.DST))
+    k = [5, 2**200 + 17]
+    sc = np.array([WL.scalar_limbs(x) for x in k], dtype=np.uint64)
+    s = WL.g1_mul(h[:2], sc)
+    for i in range(2):
+        assert list(s[i]) == B.g1_to_mont_u64(B.g1_mul(B.hash_to_g1(msgs[i], W.DST), k[i]))
+    pk = WL.g2_mul_gen(sc)
+    for i in range(2):
+        q = B.g2_mul(B.G2_GEN, k[i])
+        assert list(pk[i]) == W.g2_affine_u64(q)
+        assert bytes(WL.g2_compress(pk[i:i + 1])[0]) == B.g2_compress(q)
+        assert B.g2_decompress(B.g2_compress(q)) == (B.ST_OK, q)
+        assert list(WL.g2_prepare(pk[i:i + 1])[0]) == B.coeffs_to_limbs(B.g2_prepare(q))
+    comp = WL.g1_compress(s)
+    for i in range(2):
+        assert bytes(comp[i]) == B.g1_compress(B.g1_from_mont_u64(s[i]))
+
+
+def test_generator_configs_verify_as_expected():
+    import workload as WL
+    g2 = np.array(B.coeffs_to_limbs(B.g2_prepare(B.G2_GEN)), dtype=np.uint64)
+    c = WL.config_keyset(256, 40, seed=2)
+    r = C.verify_batch(c["sigs"], c["nhms"], g2, c["pk_tables"], pk_index=c["pk_index"], nthreads=8)
+    assert (r == c["expect"]).all() and (r == 0).sum() == 32
+    cc = WL.config_compressed(512, 40, seed=3, invalid_frac=0.05)
+    r = C.verify_compressed_batch(cc["sigs_compressed"].reshape(-1), cc["nhms"], g2, cc["pk_tables"],
+                                  pk_index=cc["pk_index"], nthreads=8)
+    assert (r == cc["expect"]).all()
+    assert set(np.unique(r[r < 0])) == {-1, -2, -3, -4}

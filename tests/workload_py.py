@@ -1,76 +1,26 @@
-"""Seeded BLS inputs built with the Python oracle, for small test cases.
-
-The generation rules match the workload generator the bench uses (SplitMix64
-stream, scalars by rejection in [1, r), 32-byte messages, RFC 9380 hash with the
-bench domain string, 1-in-8 corruptions), so small cases here and the bench's
-inputs come from one definition.
-"""
+"""Small test inputs: the bench's workload generator (icp-gpu_b200/workload.py)
+plus invalid encodings built with the Python oracle."""
 import numpy as np
 
 import bls_ref as B
 
-DST = b"BLS_BENCH_G1_XMD:SHA-256_SVDW_RO_"
-M64 = (1 << 64) - 1
+import workload as WL
 
-
-class SplitMix64:
-    def __init__(self, seed):
-        self.s = seed & M64
-
-    def next(self):
-        self.s = (self.s + 0x9E3779B97F4A7C15) & M64
-        z = self.s
-        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
-        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
-        return z ^ (z >> 31)
-
-    def scalar(self):
-        while True:
-            v = 0
-            for i in range(4):
-                v |= self.next() << (64 * i)
-            v &= (1 << 255) - 1
-            if 0 < v < B.R_ORDER:
-                return v
-
-    def msg(self):
-        return b"".join(self.next().to_bytes(8, "little") for _ in range(4))
-
-    def below(self, n):
-        return self.next() % n
+DST = WL.DST
+SplitMix64 = WL.SplitMix64
 
 
 def g2_affine_u64(q):
     return B.mont_limbs(q[0][0]) + B.mont_limbs(q[0][1]) + B.mont_limbs(q[1][0]) + B.mont_limbs(q[1][1])
 
 
-def plain_config(n=64, seed=1, corrupt_every=8):
-    """n independent keys, one message each; item i with i % corrupt_every ==
-    corrupt_every - 1 gets a one-bit message flip (expected reject)."""
-    rng = SplitMix64(seed)
-    sigs, nhms, pk_tabs, pk_aff, expect, sig_pts = [], [], [], [], [], []
-    for i in range(n):
-        sk = rng.scalar()
-        msg = rng.msg()
-        pk = B.g2_mul(B.G2_GEN, sk)
-        h = B.hash_to_g1(msg, DST)
-        sig = B.g1_mul(h, sk)
-        ok = True
-        if corrupt_every and i % corrupt_every == corrupt_every - 1:
-            m2 = bytearray(msg)
-            m2[rng.below(32)] ^= 1 << rng.below(8)
-            h = B.hash_to_g1(bytes(m2), DST)
-            ok = False
-        sigs.append(B.g1_to_mont_u64(sig))
-        sig_pts.append(sig)
-        nhms.append(B.g1_to_mont_u64(B.g1_neg(h)))
-        pk_tabs.append(B.coeffs_to_limbs(B.g2_prepare(pk)))
-        pk_aff.append(g2_affine_u64(pk))
-        expect.append(1 if ok else 0)
+def plain_config(n=64, seed=1):
+    """configs[0] from the workload generator, plus the signatures as oracle
+    points (for encoding tests)."""
+    c = WL.config_plain(n, seed)
     return {
-        "sigs": np.array(sigs, dtype=np.uint64), "nhms": np.array(nhms, dtype=np.uint64),
-        "pk_tabs": np.array(pk_tabs, dtype=np.uint64), "pk_affine": np.array(pk_aff, dtype=np.uint64),
-        "expect": np.array(expect, dtype=np.int32), "sig_points": sig_pts,
+        "sigs": c["sigs"], "nhms": c["nhms"], "pk_tabs": c["pk_tables"], "pk_affine": c["pk_affine"],
+        "expect": c["expect"], "sig_points": [B.g1_from_mont_u64(s) for s in c["sigs"]],
     }
 
 
