@@ -210,7 +210,7 @@ def run_gpu(args):
         pg = dist
 
     wl = WL.config_keyset(N_ITEMS, N_KEYS, seed=SEED + rank)
-    ctx = G.Context(device=local)
+    ctx = G.Context(device=local, lanes=args.lanes)
     ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
     for i in (0, N_KEYS - 1):  # device tables == caller-built tables
         assert (ctx.pk_table(int(ids[i])) == wl["pk_tables"][i]).all()
@@ -298,7 +298,8 @@ def run_gpu(args):
             "peak_basis": "%d SMs x 64 IMAD/clk x %.0f MHz (median SM clock sampled during the timed region)"
                           % (sms, clk),
             "imad_per_verify": IMAD_PER_VERIFY, "fp_muls_per_verify": FP_MULS_PER_VERIFY,
-            "kernel": "k_verify", "kernel_ms": round(kernel_ms, 4),
+            "kernel": "k_verify_lanes<%d>" % args.lanes if args.lanes > 1 else "k_verify",
+            "kernel_ms": round(kernel_ms, 4),
         }
         result = {
             "metric": METRIC, "value": round(value, 1), "unit": "verifies/s", "n_gpus": world,
@@ -334,6 +335,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lanes", type=int, default=8, help="lanes per verification (1, 2, 4, 8)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

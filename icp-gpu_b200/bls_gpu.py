@@ -43,7 +43,7 @@ class GpuError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_batch", ctypes.c_int), ("max_pks", ctypes.c_int),
                 ("mem_cap_bytes", ctypes.c_size_t), ("threads_per_block", ctypes.c_int),
-                ("blocks_per_sm", ctypes.c_int)]
+                ("blocks_per_sm", ctypes.c_int), ("lanes_per_pairing", ctypes.c_int)]
 
 
 class Batch(ctypes.Structure):
@@ -160,7 +160,7 @@ def g1_decompress_batch(compressed_points):
 class Context:
     """A device context: stream, buffers and resident public-key tables."""
 
-    def __init__(self, device=0, max_batch=0, max_pks=0, mem_cap_bytes=0):
+    def __init__(self, device=0, max_batch=0, max_pks=0, mem_cap_bytes=0, lanes=0, blocks_per_sm=0):
         L = lib()
         cfg = Config()
         L.bls_config_default(ctypes.byref(cfg), device)
@@ -169,6 +169,8 @@ class Context:
         if max_pks:
             cfg.max_pks = max_pks
         cfg.mem_cap_bytes = mem_cap_bytes
+        cfg.lanes_per_pairing = lanes
+        cfg.blocks_per_sm = blocks_per_sm
         h = ctypes.c_void_p()
         rc = L.bls_ctx_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != BLS_OK:

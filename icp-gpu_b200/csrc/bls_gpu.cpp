@@ -64,6 +64,7 @@ const uint64_t kG2Gen[24] = {
 struct bls_ctx {
     bls_config cfg{};
     cudaStream_t stream = nullptr;
+    int sms = 0;
     std::mutex mu;
     size_t dev_bytes = 0;  // bytes held on the device by this context
 
@@ -134,12 +135,17 @@ int ctx_init(bls_ctx* c, const bls_config* cfg) {
     c->cfg = *cfg;
     if (c->cfg.max_batch <= 0) c->cfg.max_batch = 65536;
     if (c->cfg.max_pks <= 0) c->cfg.max_pks = 1024;
+    if (c->cfg.lanes_per_pairing <= 0) c->cfg.lanes_per_pairing = 8;
+    int l = c->cfg.lanes_per_pairing;
+    if (l != 1 && l != 2 && l != 4 && l != 8)
+        return fail(BLS_ERR_INVALID, "lanes_per_pairing must be 1, 2, 4 or 8 (got %d)", l);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return fail(BLS_ERR_NODEV, "no CUDA device");
     if (c->cfg.device < 0 || c->cfg.device >= count)
         return fail(BLS_ERR_INVALID, "device %d out of range (%d devices)", c->cfg.device, count);
     CK(cudaSetDevice(c->cfg.device));
+    CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     size_t pk_bytes = (size_t)c->cfg.max_pks * bls::kCoeffU64 * 8;
     size_t need = pk_bytes + c->cfg.max_pks + bls::kCoeffU64 * 8 + 24 * 8;
@@ -183,8 +189,25 @@ int default_ctx(bls_ctx** out) {
     return BLS_OK;
 }
 
-int run_verify(bls_ctx* c, const bls::VerifyArgs& a) {
-    CK(bls::launch_verify(a, c->stream));
+// One verify launch on the context stream.  lanes_per_pairing 1 runs the
+// thread-per-verification kernel (which decodes compressed signatures itself);
+// otherwise compressed signatures are first decoded into scratch buffers by
+// one thread per point, then the lane-parallel kernel verifies.
+int run_verify(bls_ctx* c, bls::VerifyArgs a) {
+    if (c->cfg.lanes_per_pairing == 1) {
+        CK(bls::launch_verify(a, c->stream));
+        return BLS_OK;
+    }
+    const uint32_t* status = nullptr;
+    if (a.sig_compressed) {
+        int rc;
+        if ((rc = c->grow(c->d_xy, (size_t)a.n * 96)) || (rc = c->grow(c->d_st, (size_t)a.n * 4))) return rc;
+        CK(bls::launch_g1_decompress((const uint8_t*)a.sigs, a.n, (uint64_t*)c->d_xy.p, (int32_t*)c->d_st.p,
+                                     c->stream));
+        a.sig_xy = (const uint64_t*)c->d_xy.p;
+        status = (const uint32_t*)c->d_st.p;
+    }
+    CK(bls::launch_verify_lanes(a, status, c->cfg.lanes_per_pairing, c->cfg.blocks_per_sm, c->sms, c->stream));
     return BLS_OK;
 }
 

@@ -42,7 +42,6 @@ struct fp { uint32_t w[12]; };
 
 __host__ __device__ __forceinline__ fp fp_zero() {
     fp r;
-#pragma unroll
     for (int i = 0; i < 12; ++i) r.w[i] = 0;
     return r;
 }
@@ -185,6 +184,30 @@ __device__ __forceinline__ void reduce_once(uint32_t* t) {
 // ---------------------------------------------------------------------------
 // field operations
 // ---------------------------------------------------------------------------
+// Montgomery product without the final subtraction.  For a, b < 8p (the
+// redundant range of the lane-parallel kernel) the result is below 7.5p and
+// every intermediate stays below 2^416, so thirteen limbs hold it.
+__device__ __forceinline__ fp fp_mul_redundant(const fp& a, const fp& b) {
+    uint32_t t[13];
+#pragma unroll
+    for (int i = 0; i < 13; ++i) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        chain_lo(t, a.w, b.w[i]);
+        chain_hi(t, a.w, b.w[i]);
+        uint32_t m = t[0] * BLS_NINV;
+        chain_lo_p(t, m);
+        chain_hi_p(t, m);
+#pragma unroll
+        for (int j = 0; j < 12; ++j) t[j] = t[j + 1];
+        t[12] = 0;
+    }
+    fp r;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) r.w[i] = t[i];
+    return r;
+}
+
 __device__ __forceinline__ fp fp_mul(const fp& a, const fp& b) {
     uint32_t t[13];
 #pragma unroll

@@ -29,7 +29,7 @@ __device__ __forceinline__ fp fp_four() {
 }
 
 // a^((p+1)/4); a square root whenever one exists (p = 3 mod 4)
-__device__ __noinline__ fp fp_sqrt_candidate(const fp& a) {
+static __device__ __noinline__ fp fp_sqrt_candidate(const fp& a) {
     const uint64_t e[6] = {0xee7fbfffffffeaabULL, 0x07aaffffac54ffffULL, 0xd9cc34a83dac3d89ULL,
                            0xd91dd2e13ce144afULL, 0x92c6e9ed90d2eb35ULL, 0x0680447a8e5ff9a6ULL};
     return fp_pow_u64(a, e, 379);
@@ -54,7 +54,7 @@ __device__ __forceinline__ bool fp_lex_largest(const fp& a) {
 struct g1j { fp X, Y, Z; };
 
 // dbl-2009-l (a = 0)
-__device__ __noinline__ g1j g1j_dbl(const g1j& p) {
+static __device__ __noinline__ g1j g1j_dbl(const g1j& p) {
     fp A = fp_sqr(p.X), B = fp_sqr(p.Y), C = fp_sqr(B);
     fp D = fp_sub(fp_sub(fp_sqr(fp_add(p.X, B)), A), C);
     D = fp_add(D, D);
@@ -71,7 +71,7 @@ __device__ __noinline__ g1j g1j_dbl(const g1j& p) {
 }
 
 // p + (qx, qy) with q affine (madd-2007-bl), exceptional cases handled
-__device__ __noinline__ g1j g1j_add_affine(const g1j& p, const fp& qx, const fp& qy) {
+static __device__ __noinline__ g1j g1j_add_affine(const g1j& p, const fp& qx, const fp& qy) {
     if (fp_is_zero(p.Z)) return {qx, qy, fp_one()};
     fp Z1Z1 = fp_sqr(p.Z);
     fp U2 = fp_mul(qx, Z1Z1);
@@ -97,7 +97,7 @@ __device__ __noinline__ g1j g1j_add_affine(const g1j& p, const fp& qx, const fp&
 }
 
 // phi(P) == -[x^2] P for an affine curve point P (not the identity)
-__device__ __noinline__ bool g1_in_subgroup(const fp& x, const fp& y) {
+static __device__ __noinline__ bool g1_in_subgroup(const fp& x, const fp& y) {
     // x^2 = 0xac45a4010001a402_0000000100000000 (128 bits, 17 set)
     const uint64_t k[2] = {0x0000000100000000ULL, 0xac45a4010001a402ULL};
     g1j acc = {x, y, fp_one()};

@@ -17,7 +17,7 @@ __device__ __forceinline__ void store_fp2(uint64_t* p, const fp2& a) {
     fp_store_u64(p + 6, a.c1);
 }
 
-__device__ __noinline__ void g2_doubling_step(g2proj& r, uint64_t* out) {
+static __device__ __noinline__ void g2_doubling_step(g2proj& r, uint64_t* out) {
     fp2 tmp0 = fp2_sqr(r.x);
     fp2 tmp1 = fp2_sqr(r.y);
     fp2 tmp2 = fp2_sqr(tmp1);
@@ -40,7 +40,7 @@ __device__ __noinline__ void g2_doubling_step(g2proj& r, uint64_t* out) {
     store_fp2(out + 24, tmp6);
 }
 
-__device__ __noinline__ void g2_addition_step(g2proj& r, const fp2& qx, const fp2& qy, uint64_t* out) {
+static __device__ __noinline__ void g2_addition_step(g2proj& r, const fp2& qx, const fp2& qy, uint64_t* out) {
     fp2 zsq = fp2_sqr(r.z);
     fp2 ysq = fp2_sqr(qy);
     fp2 t0 = fp2_mul(zsq, qx);
@@ -66,7 +66,7 @@ __device__ __noinline__ void g2_addition_step(g2proj& r, const fp2& qx, const fp
 }
 
 // 68 coefficients of Q = (qx, qy) into out[0..2447]
-__device__ __noinline__ void g2_prepare(const fp2& qx, const fp2& qy, uint64_t* out) {
+static __device__ __noinline__ void g2_prepare(const fp2& qx, const fp2& qy, uint64_t* out) {
     g2proj r = {qx, qy, fp2_one()};
     int ci = 0;
     bool found = false;

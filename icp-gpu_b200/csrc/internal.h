@@ -20,10 +20,15 @@ struct VerifyArgs {
     int32_t* results;            // n, device
     uint64_t* ml_out;            // n x 72 or NULL, device
     uint64_t* gt_out;            // n x 72 or NULL, device
+    const uint64_t* sig_xy;      // decoded signatures (n x 12 u64) when sigs were compressed, device
 };
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
 cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStream_t s);
+// lane-parallel verify (verify_vm.cu); in_status: per-item decode status or NULL
+cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int blocks_per_sm,
+                                int sms, cudaStream_t s);
+size_t verify_lanes_smem_bytes(int lanes);
 
 }  // namespace bls

@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(64) k_g2_prepare(const uint64_t* q, int n, uin
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s) {
     if (a.n <= 0) return cudaSuccess;
+    if (a.sig_xy) return cudaErrorInvalidValue;
     int blocks = (a.n + kVerifyThreads - 1) / kVerifyThreads;
     k_verify<<<blocks, kVerifyThreads, 0, s>>>(a);
     return cudaGetLastError();

@@ -30,7 +30,7 @@ __device__ __forceinline__ void line_eval(fp12& f, const uint64_t* __restrict__ 
 // prod over both pairs of the Miller function, then conjugate (x < 0).
 // A pair whose `skip` is set contributes nothing, the ic_bls12_381 rule for
 // an identity point on either side.
-__device__ __noinline__ fp12 miller_loop_2(const fp& p1x, const fp& p1y, const uint64_t* q1, bool skip1,
+static __device__ __noinline__ fp12 miller_loop_2(const fp& p1x, const fp& p1y, const uint64_t* q1, bool skip1,
                                            const fp& p2x, const fp& p2y, const uint64_t* q2, bool skip2) {
     fp12 f = fp12_one();
     int ci = 0;
@@ -56,7 +56,7 @@ __device__ __noinline__ fp12 miller_loop_2(const fp& p1x, const fp& p1y, const u
 // f^x (x negative): square-and-multiply over |x| with the cyclotomic square,
 // then conjugate (api.cu:54-63).  The leading 1 bit starts from t = f instead
 // of multiplying 1 by f; both give the same value.
-__device__ __noinline__ fp12 cyc_exp(const fp12& f) {
+static __device__ __noinline__ fp12 cyc_exp(const fp12& f) {
     fp12 t = f;
     for (int i = 62; i >= 0; --i) {
         t = fp12_cyclotomic_sqr(t);
@@ -67,7 +67,7 @@ __device__ __noinline__ fp12 cyc_exp(const fp12& f) {
 
 // api.cu:65-78: easy part f^((p^6-1)(p^2+1)), then the hard-part chain of
 // ic_bls12_381 (same exponent, so the same Gt element bit for bit).
-__device__ __noinline__ fp12 final_exponentiation(const fp12& fi) {
+static __device__ __noinline__ fp12 final_exponentiation(const fp12& fi) {
     fp12 f = fi;
     fp12 t0 = fp12_conj(f);
     fp12 t1 = fp12_inv(f);

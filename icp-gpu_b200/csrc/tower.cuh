@@ -29,29 +29,29 @@ __device__ __forceinline__ fp2 fp2_dbl(const fp2& a) { return fp2_add(a, a); }
 __device__ __forceinline__ fp2 fp2_mul_nr(const fp2& a) { return {fp_sub(a.c0, a.c1), fp_add(a.c0, a.c1)}; }
 __device__ __forceinline__ bool fp2_is_zero(const fp2& a) { return fp_is_zero(a.c0) && fp_is_zero(a.c1); }
 
-__device__ __noinline__ fp2 fp2_mul_fp(const fp2& a, const fp& s) { return {fp_mul(a.c0, s), fp_mul(a.c1, s)}; }
+static __device__ __noinline__ fp2 fp2_mul_fp(const fp2& a, const fp& s) { return {fp_mul(a.c0, s), fp_mul(a.c1, s)}; }
 
 // (a0 + a1 u)(b0 + b1 u): three products (field_sppark.cuh:65-68)
-__device__ __noinline__ fp2 fp2_mul(const fp2& a, const fp2& b) {
+static __device__ __noinline__ fp2 fp2_mul(const fp2& a, const fp2& b) {
     fp t0 = fp_mul(a.c0, b.c0);
     fp t1 = fp_mul(a.c1, b.c1);
     fp t2 = fp_mul(fp_add(a.c0, a.c1), fp_add(b.c0, b.c1));
     return {fp_sub(t0, t1), fp_sub(fp_sub(t2, t0), t1)};
 }
 // (a0 + a1)(a0 - a1) + 2 a0 a1 u (field_sppark.cuh:69-78)
-__device__ __noinline__ fp2 fp2_sqr(const fp2& a) {
+static __device__ __noinline__ fp2 fp2_sqr(const fp2& a) {
     fp t = fp_mul(a.c0, a.c1);
     fp s = fp_mul(fp_add(a.c0, a.c1), fp_sub(a.c0, a.c1));
     return {s, fp_add(t, t)};
 }
 
 // Fermat a^(p-2) (field_sppark.cuh:40-50); maps 0 to 0
-__device__ __noinline__ fp fp_inv(const fp& a) {
+static __device__ __noinline__ fp fp_inv(const fp& a) {
     const uint64_t e[6] = {0xb9feffffffffaaa9ULL, 0x1eabfffeb153ffffULL, 0x6730d2a0f6b0f624ULL,
                            0x64774b84f38512bfULL, 0x4b1ba7b6434bacd7ULL, 0x1a0111ea397fe69aULL};
     return fp_pow_u64(a, e, 381);
 }
-__device__ __noinline__ fp2 fp2_inv(const fp2& a) {
+static __device__ __noinline__ fp2 fp2_inv(const fp2& a) {
     fp n = fp_add(fp_sqr(a.c0), fp_sqr(a.c1));
     fp i = fp_inv(n);
     return {fp_mul(a.c0, i), fp_neg(fp_mul(a.c1, i))};
@@ -66,7 +66,7 @@ __device__ __forceinline__ fp6 fp6_neg(const fp6& a) { return {fp2_neg(a.c0), fp
 __device__ __forceinline__ fp6 fp6_mul_by_v(const fp6& a) { return {fp2_mul_nr(a.c2), a.c0, a.c1}; }
 
 // Karatsuba over Fp2 (field_sppark.cuh:95-102)
-__device__ __noinline__ fp6 fp6_mul(const fp6& a, const fp6& b) {
+static __device__ __noinline__ fp6 fp6_mul(const fp6& a, const fp6& b) {
     fp2 aa = fp2_mul(a.c0, b.c0), bb = fp2_mul(a.c1, b.c1), cc = fp2_mul(a.c2, b.c2);
     fp2 x = fp2_mul(fp2_add(a.c1, a.c2), fp2_add(b.c1, b.c2));
     fp2 y = fp2_mul(fp2_add(a.c0, a.c1), fp2_add(b.c0, b.c1));
@@ -78,7 +78,7 @@ __device__ __noinline__ fp6 fp6_mul(const fp6& a, const fp6& b) {
     return r;
 }
 // field_sppark.cuh:104-111
-__device__ __noinline__ fp6 fp6_inv(const fp6& f) {
+static __device__ __noinline__ fp6 fp6_inv(const fp6& f) {
     fp2 c0s = fp2_sqr(f.c0), c1s = fp2_sqr(f.c1), c2s = fp2_sqr(f.c2);
     fp2 c01 = fp2_mul(f.c0, f.c1), c02 = fp2_mul(f.c0, f.c2), c12 = fp2_mul(f.c1, f.c2);
     fp2 t0 = fp2_sub(c0s, fp2_mul_nr(c12));
@@ -108,7 +108,7 @@ __device__ __forceinline__ fp2 frob_k12() {
                            0xc11b9cba40a8e8d0ULL, 0x2e3813cbe5a0de89ULL, 0x110eefda88847fafULL};
     return {fp_load_u64(a), fp_load_u64(b)};
 }
-__device__ __noinline__ fp6 fp6_frob(const fp6& f) {
+static __device__ __noinline__ fp6 fp6_frob(const fp6& f) {
     fp2 c1 = fp2_conj(f.c1), c2 = fp2_conj(f.c2);
     fp k1 = frob_k1(), k2 = frob_k2();
     // (x0 + x1 u) * (0 + k1 u) = -x1 k1 + x0 k1 u ;  (x0 + x1 u) * k2
@@ -118,7 +118,7 @@ __device__ __noinline__ fp6 fp6_frob(const fp6& f) {
 }
 
 // sparse products (field_sppark.cuh:126-134)
-__device__ __noinline__ fp6 fp6_mul_by_01(const fp6& s, const fp2& c0, const fp2& c1) {
+static __device__ __noinline__ fp6 fp6_mul_by_01(const fp6& s, const fp2& c0, const fp2& c1) {
     fp2 aa = fp2_mul(s.c0, c0), bb = fp2_mul(s.c1, c1);
     fp6 r;
     r.c0 = fp2_add(fp2_mul_nr(fp2_mul(s.c2, c1)), aa);
@@ -126,7 +126,7 @@ __device__ __noinline__ fp6 fp6_mul_by_01(const fp6& s, const fp2& c0, const fp2
     r.c2 = fp2_add(fp2_mul(s.c2, c0), bb);
     return r;
 }
-__device__ __noinline__ fp6 fp6_mul_by_1(const fp6& s, const fp2& c1) {
+static __device__ __noinline__ fp6 fp6_mul_by_1(const fp6& s, const fp2& c1) {
     return {fp2_mul_nr(fp2_mul(s.c2, c1)), fp2_mul(s.c0, c1), fp2_mul(s.c1, c1)};
 }
 
@@ -135,31 +135,31 @@ __device__ __forceinline__ fp12 fp12_one() { return {fp6_one(), fp6_zero()}; }
 __device__ __forceinline__ fp12 fp12_conj(const fp12& a) { return {a.c0, fp6_neg(a.c1)}; }
 
 // field_sppark.cuh:142-146
-__device__ __noinline__ fp12 fp12_mul(const fp12& a, const fp12& b) {
+static __device__ __noinline__ fp12 fp12_mul(const fp12& a, const fp12& b) {
     fp6 aa = fp6_mul(a.c0, b.c0), bb = fp6_mul(a.c1, b.c1);
     fp6 s = fp6_mul(fp6_add(a.c0, a.c1), fp6_add(b.c0, b.c1));
     return {fp6_add(aa, fp6_mul_by_v(bb)), fp6_sub(fp6_sub(s, aa), bb)};
 }
 // field_sppark.cuh:148-151
-__device__ __noinline__ fp12 fp12_sqr(const fp12& a) {
+static __device__ __noinline__ fp12 fp12_sqr(const fp12& a) {
     fp6 ab = fp6_mul(a.c0, a.c1);
     fp6 s = fp6_mul(fp6_add(a.c0, fp6_mul_by_v(a.c1)), fp6_add(a.c0, a.c1));
     return {fp6_sub(fp6_sub(s, ab), fp6_mul_by_v(ab)), fp6_add(ab, ab)};
 }
 // field_sppark.cuh:153-157
-__device__ __noinline__ fp12 fp12_inv(const fp12& f) {
+static __device__ __noinline__ fp12 fp12_inv(const fp12& f) {
     fp6 t = fp6_sub(fp6_mul(f.c0, f.c0), fp6_mul_by_v(fp6_mul(f.c1, f.c1)));
     fp6 ti = fp6_inv(t);
     return {fp6_mul(f.c0, ti), fp6_neg(fp6_mul(f.c1, ti))};
 }
 // field_sppark.cuh:159-166
-__device__ __noinline__ fp12 fp12_frob(const fp12& f) {
+static __device__ __noinline__ fp12 fp12_frob(const fp12& f) {
     fp6 c0 = fp6_frob(f.c0), c1 = fp6_frob(f.c1);
     fp2 k = frob_k12();
     return {c0, {fp2_mul(c1.c0, k), fp2_mul(c1.c1, k), fp2_mul(c1.c2, k)}};
 }
 // f * (c0 + c1 v + c4 v w)  (field_sppark.cuh:168-172)
-__device__ __noinline__ fp12 fp12_mul_by_014(const fp12& f, const fp2& c0, const fp2& c1, const fp2& c4) {
+static __device__ __noinline__ fp12 fp12_mul_by_014(const fp12& f, const fp2& c0, const fp2& c1, const fp2& c4) {
     fp6 aa = fp6_mul_by_01(f.c0, c0, c1);
     fp6 bb = fp6_mul_by_1(f.c1, c4);
     fp6 t = fp6_mul_by_01(fp6_add(f.c1, f.c0), c0, fp2_add(c1, c4));
@@ -172,7 +172,7 @@ __device__ __forceinline__ void fp4_square(const fp2& a, const fp2& b, fp2& o0, 
     o0 = fp2_add(fp2_mul_nr(t1), t0);
     o1 = fp2_sub(fp2_sub(fp2_sqr(fp2_add(a, b)), t0), t1);
 }
-__device__ __noinline__ fp12 fp12_cyclotomic_sqr(const fp12& f) {
+static __device__ __noinline__ fp12 fp12_cyclotomic_sqr(const fp12& f) {
     fp2 z0 = f.c0.c0, z4 = f.c0.c1, z3 = f.c0.c2, z2 = f.c1.c0, z1 = f.c1.c1, z5 = f.c1.c2;
     fp2 A0, A1, B0, B1, C0, C1;
     fp4_square(z0, z1, A0, A1);

@@ -112,6 +112,8 @@ typedef struct {
     size_t mem_cap_bytes;   /* device-memory budget for this context (0 = none) */
     int threads_per_block;  /* 0 = library default */
     int blocks_per_sm;      /* persistent launches: 0 = occupancy maximum */
+    int lanes_per_pairing;  /* 1: one thread per verification; 2, 4, 8: that many lanes
+                               share one verification (0 = 8) */
 } bls_config;
 
 typedef struct {

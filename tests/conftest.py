@@ -5,7 +5,7 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-for sub in ("", "oracle", "icp-gpu_b200", "tests"):
+for sub in ("", "oracle", "icp-gpu_b200", "icp-gpu_b200/csrc", "tests"):
     p = os.path.join(ROOT, sub)
     if p not in sys.path:
         sys.path.insert(0, p)

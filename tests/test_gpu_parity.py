@@ -11,10 +11,10 @@ import workload_py as W
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def ctx():
+@pytest.fixture(scope="module", params=[8, 4, 1], ids=["lanes8", "lanes4", "thread"])
+def ctx(request):
     G.init()
-    with G.Context() as c:
+    with G.Context(lanes=request.param) as c:
         yield c
 
 
