@@ -287,6 +287,10 @@ def run_gpu(args):
         e2e_s = float(t.item())
     e2e_value = N_ITEMS * world * args.steps / e2e_s
 
+    batching = None
+    if not args.no_extras:
+        batching = run_batching(G, WL, ctx, ids)
+
     result = None
     if rank == 0:
         clk = clocks["sm_mhz"] or float(load_peaks().get("sm_max_mhz", 1965.0))
@@ -318,6 +322,8 @@ def run_gpu(args):
             "gpu_launches": args.steps,
             "bit_exact": True,
         }
+        if batching:
+            result["batching"] = batching
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(wl, generator_table(WL))
     ctx.close()
@@ -328,6 +334,30 @@ def run_gpu(args):
         print(json.dumps(result), flush=True)
 
 
+def run_batching(G, WL, ctx, ids_unused, reps=2):
+    """configs[3]: 256 requests, sizes log-uniform in [1, 2048], 1-40 keys each;
+    one launch per request against one persistent graph-replayed launch, both
+    through bls_verify_requests from host buffers (host-timed, best of reps)."""
+    wl = WL.config_requests(256, 2048, N_KEYS, seed=4)
+    ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
+    off = wl["offsets"]
+    reqs = [(wl["sigs"][a:b], wl["nhms"][a:b], ids[wl["pk_index"][a:b]]) for a, b in zip(off[:-1], off[1:])]
+    n = int(off[-1])
+    out = {"requests": len(reqs), "items": n, "sizes": "log-uniform [1, 2048]"}
+    for mode, name in ((G.MODE_PLAIN, "plain"), (G.MODE_PERSISTENT, "persistent")):
+        r = ctx.verify_requests(reqs, mode=mode)
+        assert (np.concatenate(r) == wl["expect"]).all(), "batched accept bits differ"
+        best = 1e30
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            ctx.verify_requests(reqs, mode=mode)
+            best = min(best, time.perf_counter() - t0)
+        out[name + "_verifies_per_s"] = round(n / best, 1)
+        out[name + "_ms"] = round(best * 1e3, 2)
+    out["speedup"] = round(out["persistent_verifies_per_s"] / out["plain_verifies_per_s"], 2)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -335,6 +365,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batching and serving sections")
     ap.add_argument("--lanes", type=int, default=8, help="lanes per verification (1, 2, 4, 8)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -46,6 +46,18 @@ class Config(ctypes.Structure):
                 ("blocks_per_sm", ctypes.c_int), ("lanes_per_pairing", ctypes.c_int)]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("sigs", ctypes.c_void_p), ("neg_hms", ctypes.c_void_p),
+                ("pk_ids", ctypes.c_void_p), ("results", ctypes.c_void_p)]
+
+
+class TunePoint(ctypes.Structure):
+    _fields_ = [("lanes_per_pairing", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("ms", ctypes.c_float)]
+
+
+MODE_PLAIN, MODE_PERSISTENT = 0, 1
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("sig_format", ctypes.c_int), ("sigs", ctypes.c_void_p),
                 ("neg_hms", ctypes.c_void_p), ("pk_ids", ctypes.c_void_p),
@@ -85,6 +97,8 @@ def lib():
         L.bls_ctx_stream.argtypes = [P]
         L.bls_ctx_stream.restype = P
         L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
+        L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
+        L.bls_autotune.argtypes = [P, ctypes.POINTER(Batch), I, ctypes.POINTER(TunePoint), I, ctypes.POINTER(I)]
         _lib = L
     return _lib
 
@@ -253,3 +267,32 @@ class Context:
         self._check(self.lib.bls_g1_decompress_status(self.h, _ptr(src), n, _ptr(xy), _ptr(st)),
                     "bls_g1_decompress_status")
         return st, xy
+
+    def verify_requests(self, requests, compressed=False, mode=MODE_PERSISTENT):
+        """requests: list of (sigs, neg_hms, pk_ids); returns a list of int32
+        result arrays.  MODE_PLAIN launches once per request; MODE_PERSISTENT
+        runs all of them in one graph-replayed persistent launch."""
+        keep, reqs, outs = [], [], []
+        for sigs, nhms, ids in requests:
+            nhms = _u64(nhms, 12)
+            n = nhms.shape[0]
+            s = (np.ascontiguousarray(sigs, dtype=np.uint8).reshape(-1) if compressed else _u64(sigs, 12))
+            ids = np.ascontiguousarray(ids, dtype=np.int32).reshape(-1)
+            res = np.zeros(n, dtype=np.int32)
+            keep += [s, nhms, ids]
+            outs.append(res)
+            reqs.append(Request(n, _ptr(s), _ptr(nhms), _ptr(ids), _ptr(res)))
+        arr = (Request * max(1, len(reqs)))(*reqs)
+        self._check(self.lib.bls_verify_requests(self.h, arr, len(reqs), SIG_COMPRESSED if compressed else SIG_AFFINE,
+                                                 mode), "bls_verify_requests")
+        return outs
+
+    def autotune(self, n, sigs_ptr, nhms_ptr, ids_ptr, compressed=False, repeats=3):
+        """Time every kernel configuration on a device-resident sample and keep
+        the fastest; returns [(lanes, blocks_per_sm, ms), ...]."""
+        b = Batch(n, SIG_COMPRESSED if compressed else SIG_AFFINE, sigs_ptr, nhms_ptr, ids_ptr, None, None)
+        pts = (TunePoint * 32)()
+        npts = ctypes.c_int()
+        self._check(self.lib.bls_autotune(self.h, ctypes.byref(b), repeats, pts, 32, ctypes.byref(npts)),
+                    "bls_autotune")
+        return [(pts[i].lanes_per_pairing, pts[i].blocks_per_sm, pts[i].ms) for i in range(npts.value)]

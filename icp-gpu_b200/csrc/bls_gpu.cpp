@@ -77,8 +77,13 @@ struct bls_ctx {
         size_t cap = 0;
     };
     // per-call scratch
-    DevBuf d_sigs, d_nhms, d_pkidx, d_res, d_ml, d_gt, d_pk_items, d_g2_call, d_in, d_xy, d_st;
+    DevBuf d_sigs, d_nhms, d_pkidx, d_res, d_ml, d_gt, d_pk_items, d_g2_call, d_in, d_xy, d_st, d_work;
     HostBuf h_sigs, h_nhms, h_pkidx, h_res;
+
+    // persistent batched launch captured as a CUDA graph, valid while the
+    // item count, format and every buffer address stay the same
+    cudaGraphExec_t graph = nullptr;
+    std::vector<const void*> graph_key;
 
     // registered tables
     uint64_t* d_g2 = nullptr;       // generator table
@@ -116,9 +121,15 @@ struct bls_ctx {
         b.cap = want;
         return BLS_OK;
     }
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_key.clear();
+    }
     void release() {
+        drop_graph();
         for (DevBuf* b : {&d_sigs, &d_nhms, &d_pkidx, &d_res, &d_ml, &d_gt, &d_pk_items, &d_g2_call, &d_in,
-                          &d_xy, &d_st})
+                          &d_xy, &d_st, &d_work})
             if (b->p) cudaFree(b->p);
         for (HostBuf* b : {&h_sigs, &h_nhms, &h_pkidx, &h_res})
             if (b->p) cudaFreeHost(b->p);
@@ -195,19 +206,70 @@ int default_ctx(bls_ctx** out) {
 // one thread per point, then the lane-parallel kernel verifies.
 int run_verify(bls_ctx* c, bls::VerifyArgs a) {
     if (c->cfg.lanes_per_pairing == 1) {
+        a.work_counter = nullptr;
         CK(bls::launch_verify(a, c->stream));
         return BLS_OK;
     }
     const uint32_t* status = nullptr;
     if (a.sig_compressed) {
         int rc;
-        if ((rc = c->grow(c->d_xy, (size_t)a.n * 96)) || (rc = c->grow(c->d_st, (size_t)a.n * 4))) return rc;
+        if ((c->d_xy.cap < (size_t)a.n * 96 || c->d_st.cap < (size_t)a.n * 4) &&
+            ((rc = c->grow(c->d_xy, (size_t)a.n * 96)) || (rc = c->grow(c->d_st, (size_t)a.n * 4))))
+            return rc;
         CK(bls::launch_g1_decompress((const uint8_t*)a.sigs, a.n, (uint64_t*)c->d_xy.p, (int32_t*)c->d_st.p,
                                      c->stream));
         a.sig_xy = (const uint64_t*)c->d_xy.p;
         status = (const uint32_t*)c->d_st.p;
     }
+    if (a.work_counter) CK(cudaMemsetAsync(a.work_counter, 0, sizeof(int), c->stream));
     CK(bls::launch_verify_lanes(a, status, c->cfg.lanes_per_pairing, c->cfg.blocks_per_sm, c->sms, c->stream));
+    return BLS_OK;
+}
+
+// grow every buffer a verify of n staged items needs (nothing allocates after)
+int prepare(bls_ctx* c, size_t n, int fmt, bool want_ml, bool want_gt) {
+    size_t sig_bytes = n * (fmt == BLS_SIG_COMPRESSED ? 48 : 96);
+    int rc;
+    if ((rc = c->grow(c->d_sigs, sig_bytes)) || (rc = c->grow(c->d_nhms, n * 96)) ||
+        (rc = c->grow(c->d_pkidx, n * 4)) || (rc = c->grow(c->d_res, n * 4)) || (rc = c->grow(c->d_work, 256)))
+        return rc;
+    if (fmt == BLS_SIG_COMPRESSED && ((rc = c->grow(c->d_xy, n * 96)) || (rc = c->grow(c->d_st, n * 4)))) return rc;
+    if (want_ml && (rc = c->grow(c->d_ml, n * 576))) return rc;
+    if (want_gt && (rc = c->grow(c->d_gt, n * 576))) return rc;
+    if ((rc = c->grow(c->h_sigs, sig_bytes)) || (rc = c->grow(c->h_nhms, n * 96)) ||
+        (rc = c->grow(c->h_pkidx, n * 4)) || (rc = c->grow(c->h_res, n * 4)))
+        return rc;
+    return BLS_OK;
+}
+
+// enqueue: staged inputs -> device, verify, results -> h_res (no synchronise)
+int enqueue(bls_ctx* c, size_t n, int fmt, bool persistent, bool want_ml, bool want_gt) {
+    size_t sig_bytes = n * (fmt == BLS_SIG_COMPRESSED ? 48 : 96);
+    CK(cudaMemcpyAsync(c->d_sigs.p, c->h_sigs.p, sig_bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_nhms.p, c->h_nhms.p, n * 96, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_pkidx.p, c->h_pkidx.p, n * 4, cudaMemcpyHostToDevice, c->stream));
+    bls::VerifyArgs a{};
+    a.sigs = c->d_sigs.p;
+    a.sig_compressed = fmt == BLS_SIG_COMPRESSED;
+    a.nhms = (const uint64_t*)c->d_nhms.p;
+    a.g2 = c->d_g2;
+    a.pk_tables = c->d_pk;
+    a.pk_index = (const int32_t*)c->d_pkidx.p;
+    a.pk_identity = c->d_pk_inf;
+    a.n = (int)n;
+    a.results = (int32_t*)c->d_res.p;
+    a.ml_out = want_ml ? (uint64_t*)c->d_ml.p : nullptr;
+    a.gt_out = want_gt ? (uint64_t*)c->d_gt.p : nullptr;
+    a.work_counter = persistent ? (int*)c->d_work.p : nullptr;
+    int rc = run_verify(c, a);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->h_res.p, a.results, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    return BLS_OK;
+}
+
+int check_ids(bls_ctx* c, const int32_t* ids, int n) {
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 0 || ids[i] >= c->n_pks) return fail(BLS_ERR_INVALID, "item %d: unknown pk id %d", i, ids[i]);
     return BLS_OK;
 }
 
@@ -315,45 +377,169 @@ int bls_verify_batch(bls_ctx* ctx, const bls_batch* b, int32_t* results) {
     if (b->sig_format != BLS_SIG_AFFINE && b->sig_format != BLS_SIG_COMPRESSED)
         return fail(BLS_ERR_INVALID, "unknown sig_format %d", b->sig_format);
     std::lock_guard<std::mutex> lk(ctx->mu);
-    for (int i = 0; i < b->n; ++i)
-        if (b->pk_ids[i] < 0 || b->pk_ids[i] >= ctx->n_pks)
-            return fail(BLS_ERR_INVALID, "item %d: unknown pk id %d", i, b->pk_ids[i]);
+    int rc;
+    if ((rc = check_ids(ctx, b->pk_ids, b->n))) return rc;
     CK(cudaSetDevice(ctx->cfg.device));
     size_t n = (size_t)b->n;
     size_t sig_bytes = n * (b->sig_format == BLS_SIG_COMPRESSED ? 48 : 96);
-    int rc;
-    if ((rc = ctx->grow(ctx->d_sigs, sig_bytes)) || (rc = ctx->grow(ctx->d_nhms, n * 96)) ||
-        (rc = ctx->grow(ctx->d_pkidx, n * 4)) || (rc = ctx->grow(ctx->d_res, n * 4)))
-        return rc;
-    if (b->miller_out && (rc = ctx->grow(ctx->d_ml, n * 576))) return rc;
-    if (b->gt_out && (rc = ctx->grow(ctx->d_gt, n * 576))) return rc;
-    if ((rc = ctx->grow(ctx->h_sigs, sig_bytes)) || (rc = ctx->grow(ctx->h_nhms, n * 96)) ||
-        (rc = ctx->grow(ctx->h_pkidx, n * 4)) || (rc = ctx->grow(ctx->h_res, n * 4)))
-        return rc;
+    if ((rc = prepare(ctx, n, b->sig_format, b->miller_out != nullptr, b->gt_out != nullptr))) return rc;
     memcpy(ctx->h_sigs.p, b->sigs, sig_bytes);
     memcpy(ctx->h_nhms.p, b->neg_hms, n * 96);
     memcpy(ctx->h_pkidx.p, b->pk_ids, n * 4);
-    CK(cudaMemcpyAsync(ctx->d_sigs.p, ctx->h_sigs.p, sig_bytes, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->d_nhms.p, ctx->h_nhms.p, n * 96, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->d_pkidx.p, ctx->h_pkidx.p, n * 4, cudaMemcpyHostToDevice, ctx->stream));
-    bls::VerifyArgs a{};
-    a.sigs = ctx->d_sigs.p;
-    a.sig_compressed = b->sig_format == BLS_SIG_COMPRESSED;
-    a.nhms = (const uint64_t*)ctx->d_nhms.p;
-    a.g2 = ctx->d_g2;
-    a.pk_tables = ctx->d_pk;
-    a.pk_index = (const int32_t*)ctx->d_pkidx.p;
-    a.pk_identity = ctx->d_pk_inf;
-    a.n = b->n;
-    a.results = (int32_t*)ctx->d_res.p;
-    a.ml_out = b->miller_out ? (uint64_t*)ctx->d_ml.p : nullptr;
-    a.gt_out = b->gt_out ? (uint64_t*)ctx->d_gt.p : nullptr;
-    if ((rc = run_verify(ctx, a))) return rc;
-    CK(cudaMemcpyAsync(ctx->h_res.p, a.results, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    if (b->miller_out) CK(cudaMemcpyAsync(b->miller_out, a.ml_out, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
-    if (b->gt_out) CK(cudaMemcpyAsync(b->gt_out, a.gt_out, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
+    if ((rc = enqueue(ctx, n, b->sig_format, false, b->miller_out != nullptr, b->gt_out != nullptr))) return rc;
+    if (b->miller_out) CK(cudaMemcpyAsync(b->miller_out, ctx->d_ml.p, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
+    if (b->gt_out) CK(cudaMemcpyAsync(b->gt_out, ctx->d_gt.p, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     memcpy(results, ctx->h_res.p, n * 4);
+    return BLS_OK;
+}
+
+int bls_verify_requests(bls_ctx* ctx, const bls_request* reqs, int nreq, int fmt, int mode) {
+    if (!ctx || (!reqs && nreq > 0)) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (nreq < 0) return fail(BLS_ERR_INVALID, "nreq < 0");
+    if (fmt != BLS_SIG_AFFINE && fmt != BLS_SIG_COMPRESSED) return fail(BLS_ERR_INVALID, "unknown sig_format %d", fmt);
+    if (mode != BLS_MODE_PLAIN && mode != BLS_MODE_PERSISTENT) return fail(BLS_ERR_INVALID, "unknown mode %d", mode);
+    size_t total = 0;
+    for (int r = 0; r < nreq; ++r) {
+        if (reqs[r].n < 0) return fail(BLS_ERR_INVALID, "request %d: n < 0", r);
+        if (reqs[r].n && (!reqs[r].sigs || !reqs[r].neg_hms || !reqs[r].pk_ids || !reqs[r].results))
+            return fail(BLS_ERR_INVALID, "request %d: NULL array", r);
+        total += (size_t)reqs[r].n;
+    }
+    if (total == 0) return BLS_OK;
+    if (total > (size_t)INT32_MAX) return fail(BLS_ERR_INVALID, "too many items");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int rc;
+    for (int r = 0; r < nreq; ++r)
+        if ((rc = check_ids(ctx, reqs[r].pk_ids, reqs[r].n))) return rc;
+    CK(cudaSetDevice(ctx->cfg.device));
+    const size_t sb = fmt == BLS_SIG_COMPRESSED ? 48 : 96;
+    if (mode == BLS_MODE_PLAIN) {
+        for (int r = 0; r < nreq; ++r) {
+            size_t n = (size_t)reqs[r].n;
+            if (!n) continue;
+            if ((rc = prepare(ctx, n, fmt, false, false))) return rc;
+            memcpy(ctx->h_sigs.p, reqs[r].sigs, n * sb);
+            memcpy(ctx->h_nhms.p, reqs[r].neg_hms, n * 96);
+            memcpy(ctx->h_pkidx.p, reqs[r].pk_ids, n * 4);
+            if ((rc = enqueue(ctx, n, fmt, false, false, false))) return rc;
+            CK(cudaStreamSynchronize(ctx->stream));
+            memcpy(reqs[r].results, ctx->h_res.p, n * 4);
+        }
+        return BLS_OK;
+    }
+    if ((rc = prepare(ctx, total, fmt, false, false))) return rc;
+    size_t off = 0;
+    for (int r = 0; r < nreq; ++r) {
+        size_t n = (size_t)reqs[r].n;
+        memcpy((char*)ctx->h_sigs.p + off * sb, reqs[r].sigs, n * sb);
+        memcpy((char*)ctx->h_nhms.p + off * 96, reqs[r].neg_hms, n * 96);
+        memcpy((char*)ctx->h_pkidx.p + off * 4, reqs[r].pk_ids, n * 4);
+        off += n;
+    }
+    std::vector<const void*> key = {(const void*)total, (const void*)(size_t)fmt,
+                                    (const void*)(size_t)ctx->cfg.lanes_per_pairing,
+                                    (const void*)(size_t)ctx->cfg.blocks_per_sm, ctx->d_sigs.p, ctx->d_nhms.p,
+                                    ctx->d_pkidx.p, ctx->d_res.p, ctx->d_work.p, ctx->d_xy.p, ctx->d_st.p,
+                                    ctx->h_sigs.p, ctx->h_nhms.p, ctx->h_pkidx.p, ctx->h_res.p};
+    if (!ctx->graph || ctx->graph_key != key) {
+        ctx->drop_graph();
+        if (ctx->cfg.lanes_per_pairing > 1) bls::verify_lanes_blocks_per_sm(ctx->cfg.lanes_per_pairing);  // set up outside capture
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue(ctx, total, fmt, true, false, false);
+        cudaError_t ec = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ec != cudaSuccess) return fail(BLS_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
+        ec = cudaGraphInstantiate(&ctx->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ec != cudaSuccess) {
+            ctx->graph = nullptr;
+            return fail(BLS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ec));
+        }
+        ctx->graph_key = key;
+    }
+    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    off = 0;
+    for (int r = 0; r < nreq; ++r) {
+        memcpy(reqs[r].results, (const char*)ctx->h_res.p + off * 4, (size_t)reqs[r].n * 4);
+        off += (size_t)reqs[r].n;
+    }
+    return BLS_OK;
+}
+
+int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* points, int max_points,
+                 int* n_points) {
+    if (!ctx || !b || b->n <= 0) return fail(BLS_ERR_INVALID, "bad sample");
+    if (repeats <= 0) repeats = 3;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int rc;
+    if ((rc = ctx->grow(ctx->d_res, (size_t)b->n * 4)) || (rc = ctx->grow(ctx->d_work, 256))) return rc;
+    if (b->sig_format == BLS_SIG_COMPRESSED &&
+        ((rc = ctx->grow(ctx->d_xy, (size_t)b->n * 96)) || (rc = ctx->grow(ctx->d_st, (size_t)b->n * 4))))
+        return rc;
+    struct Cand { int lanes, bps; };
+    std::vector<Cand> cands;
+    cands.push_back({1, 0});
+    for (int l : {2, 4, 8}) {
+        int res = bls::verify_lanes_blocks_per_sm(l);
+        cands.push_back({l, 0});
+        for (int bps : {res - 1, res / 2})
+            if (bps >= 1 && bps < res) cands.push_back({l, bps});
+    }
+    bls_config saved = ctx->cfg;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    Cand bestc = {saved.lanes_per_pairing, saved.blocks_per_sm};
+    int np = 0;
+    for (const Cand& cd : cands) {
+        ctx->cfg.lanes_per_pairing = cd.lanes;
+        ctx->cfg.blocks_per_sm = cd.bps;
+        bls::VerifyArgs a{};
+        a.sigs = b->sigs;
+        a.sig_compressed = b->sig_format == BLS_SIG_COMPRESSED;
+        a.nhms = b->neg_hms;
+        a.g2 = ctx->d_g2;
+        a.pk_tables = ctx->d_pk;
+        a.pk_index = b->pk_ids;
+        a.pk_identity = ctx->d_pk_inf;
+        a.n = b->n;
+        a.results = (int32_t*)ctx->d_res.p;
+        a.work_counter = cd.lanes > 1 ? (int*)ctx->d_work.p : nullptr;
+        if ((rc = run_verify(ctx, a))) break;  // warm-up
+        float ms_best = 1e30f;
+        for (int r = 0; r < repeats && !rc; ++r) {
+            cudaEventRecord(e0, ctx->stream);
+            rc = run_verify(ctx, a);
+            cudaEventRecord(e1, ctx->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(BLS_ERR_CUDA, "autotune sync failed");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < ms_best) ms_best = ms;
+        }
+        if (rc) break;
+        if (points && np < max_points) points[np] = {cd.lanes, cd.bps, ms_best};
+        ++np;
+        if (ms_best < best) {
+            best = ms_best;
+            bestc = cd;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->cfg = saved;
+    if (rc) return rc;
+    ctx->cfg.lanes_per_pairing = bestc.lanes;
+    ctx->cfg.blocks_per_sm = bestc.bps;
+    ctx->drop_graph();
+    if (n_points) *n_points = np < max_points ? np : max_points;
     return BLS_OK;
 }
 

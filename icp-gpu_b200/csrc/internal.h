@@ -21,6 +21,7 @@ struct VerifyArgs {
     uint64_t* ml_out;            // n x 72 or NULL, device
     uint64_t* gt_out;            // n x 72 or NULL, device
     const uint64_t* sig_xy;      // decoded signatures (n x 12 u64) when sigs were compressed, device
+    int* work_counter;           // persistent mode: items are claimed from this zeroed counter, device
 };
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
@@ -30,5 +31,7 @@ cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStrea
 cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int blocks_per_sm,
                                 int sms, cudaStream_t s);
 size_t verify_lanes_smem_bytes(int lanes);
+// blocks of the lane-parallel kernel resident per SM (occupancy calculator)
+int verify_lanes_blocks_per_sm(int lanes);
 
 }  // namespace bls

@@ -213,9 +213,24 @@ __global__ void __launch_bounds__(32 * 4) k_verify_lanes(VerifyArgs a, const uin
     c.temp = c.region + vm::kGroups * vm::kGroupSlots;
     c.lane = lane32 & (T - 1);
 
-    for (int base = blockIdx.x * pairs_per_block; base < a.n; base += gridDim.x * pairs_per_block) {
-        // warp-uniform trip count: every pairing of the warp runs the programs
-        const int item = base + pair_in_block;
+    // Items are taken a warp at a time (one per pairing): from a counter in
+    // persistent mode, so uneven work balances across the resident warps, or
+    // by a fixed stride otherwise.  The trip count is warp-uniform: every
+    // pairing of the warp runs the programs, idle ones on the identity.
+    int next = (blockIdx.x * warps + warp) * kPairsPerWarp;
+    const int stride = gridDim.x * pairs_per_block;
+    for (;;) {
+        int base;
+        if (a.work_counter) {
+            int b = 0;
+            if (lane32 == 0) b = atomicAdd(a.work_counter, kPairsPerWarp);
+            base = __shfl_sync(0xffffffffu, b, 0);
+        } else {
+            base = next;
+            next += stride;
+        }
+        if (base >= a.n) break;
+        const int item = base + lane32 / T;
         const bool active = item < a.n;
         bool skip1 = true, skip2 = true;
         const uint64_t* pk = a.g2;
@@ -271,22 +286,44 @@ __global__ void __launch_bounds__(32 * 4) k_verify_lanes(VerifyArgs a, const uin
     }
 }
 
+constexpr int kWarpsPerBlock = 1;
+
+template <int T>
+size_t smem_t() {
+    return (size_t)(vm::kKSlots + kWarpsPerBlock * (32 / T) * vm::Layout<T>::kSlots) * vm::kSlotBytes;
+}
+
+template <int T>
+cudaError_t configure_t() {
+    static cudaError_t done = cudaFuncSetAttribute(k_verify_lanes<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem_t<T>());
+    return done;
+}
+
+template <int T>
+int resident_t() {
+    if (configure_t<T>() != cudaSuccess) return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_verify_lanes<T>, 32 * kWarpsPerBlock, smem_t<T>()) !=
+        cudaSuccess)
+        return 0;
+    return blocks;
+}
+
 template <int T>
 cudaError_t launch_t(const VerifyArgs& a, const uint32_t* in_status, cudaStream_t s, int blocks_per_sm, int sms) {
-    constexpr int kWarps = 1;
-    size_t smem = (size_t)(vm::kKSlots + kWarps * (32 / T) * vm::Layout<T>::kSlots) * vm::kSlotBytes;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_verify_lanes<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    int pairs_per_block = kWarps * (32 / T);
+    cudaError_t e = configure_t<T>();
+    if (e != cudaSuccess) return e;
+    int pairs_per_block = kWarpsPerBlock * (32 / T);
     int need = (a.n + pairs_per_block - 1) / pairs_per_block;
-    int cap = blocks_per_sm > 0 ? blocks_per_sm * sms : need;
-    int blocks = need < cap ? need : cap;
+    int resident = resident_t<T>();
+    int per_sm = blocks_per_sm > 0 ? blocks_per_sm : (resident > 0 ? resident : 1);
+    int cap = per_sm * sms;
+    // persistent mode: exactly the resident grid, items claimed from the counter
+    int blocks = a.work_counter ? cap : (need < cap || blocks_per_sm <= 0 ? need : cap);
+    if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
-    k_verify_lanes<T><<<blocks, 32 * kWarps, smem, s>>>(a, in_status);
+    k_verify_lanes<T><<<blocks, 32 * kWarpsPerBlock, smem_t<T>(), s>>>(a, in_status);
     return cudaGetLastError();
 }
 
@@ -294,10 +331,18 @@ cudaError_t launch_t(const VerifyArgs& a, const uint32_t* in_status, cudaStream_
 
 size_t verify_lanes_smem_bytes(int lanes) {
     switch (lanes) {
-        case 1: return (size_t)(vm::kKSlots + 32 * vm::Layout<1>::kSlots) * vm::kSlotBytes;
-        case 2: return (size_t)(vm::kKSlots + 16 * vm::Layout<2>::kSlots) * vm::kSlotBytes;
-        case 4: return (size_t)(vm::kKSlots + 8 * vm::Layout<4>::kSlots) * vm::kSlotBytes;
-        default: return (size_t)(vm::kKSlots + 4 * vm::Layout<8>::kSlots) * vm::kSlotBytes;
+        case 2: return smem_t<2>();
+        case 4: return smem_t<4>();
+        default: return smem_t<8>();
+    }
+}
+
+int verify_lanes_blocks_per_sm(int lanes) {
+    switch (lanes) {
+        case 2: return resident_t<2>();
+        case 4: return resident_t<4>();
+        case 8: return resident_t<8>();
+        default: return 0;
     }
 }
 

@@ -157,6 +157,36 @@ int bls_ctx_sync(bls_ctx* ctx);
 /* the context's CUDA stream (cudaStream_t) */
 void* bls_ctx_stream(bls_ctx* ctx);
 
+/* ---- batching (many requests, one launch) ---- */
+typedef struct {
+    int n;                     /* items in this request */
+    const void* sigs;          /* n x 12 uint64 or n x 48 bytes (format given per call) */
+    const uint64_t* neg_hms;   /* n x 12 uint64 */
+    const int32_t* pk_ids;     /* n registered key ids */
+    int32_t* results;          /* n results, as bls_verify_batch */
+} bls_request;
+
+#define BLS_MODE_PLAIN 0       /* one launch (copy in, verify, copy out) per request */
+#define BLS_MODE_PERSISTENT 1  /* all requests in one persistent launch whose warps claim
+                                  items from a device counter, captured once in a CUDA
+                                  graph and replayed while the request shapes repeat */
+
+/* Verify nreq requests (all with signatures in `sig_format`), synchronously. */
+int bls_verify_requests(bls_ctx* ctx, const bls_request* reqs, int nreq, int sig_format, int mode);
+
+/* ---- autotuning ---- */
+typedef struct {
+    int lanes_per_pairing;
+    int blocks_per_sm;          /* 0 = occupancy maximum */
+    float ms;                   /* kernel time on the sample, best of the repeats */
+} bls_tune_point;
+
+/* Time the verify kernel on a device-resident sample batch for every
+ * (lanes_per_pairing, blocks_per_sm) candidate, keep the fastest in the
+ * context, and report up to max_points measurements (returns how many). */
+int bls_autotune(bls_ctx* ctx, const bls_batch* sample_device, int repeats, bls_tune_point* points,
+                 int max_points, int* n_points);
+
 /* Decode n compressed G1 points: status[i] (BLS_ST_*), xy[i] 12 x uint64
  * (identity: x = 0, y = R mod p; failures: zeros). */
 int bls_g1_decompress_status(bls_ctx* ctx, const uint8_t* compressed, int n, uint64_t* xy, int32_t* status);
