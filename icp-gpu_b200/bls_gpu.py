@@ -98,6 +98,7 @@ def lib():
         L.bls_ctx_stream.restype = P
         L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
+        L.bls_verify_compressed_noalloc.argtypes = [P, P, P, P, P, P, I, I, P]
         L.bls_autotune.argtypes = [P, ctypes.POINTER(Batch), I, ctypes.POINTER(TunePoint), I, ctypes.POINTER(I)]
         _lib = L
     return _lib
@@ -170,6 +171,18 @@ def g1_decompress_batch(compressed_points):
 # ----------------------------------------------------------------------------
 # extended API
 # ----------------------------------------------------------------------------
+
+NOALLOC_MAX_ITEMS = 8192
+
+
+def verify_compressed_noalloc(sigs48_ptr, nhms_ptr, g2_ptr, pk_tables_ptr, pk_index_ptr, results_ptr, n,
+                              lanes=8, stream=None):
+    """Enqueue a verify of n compressed signatures on `stream` using only
+    caller-owned device buffers (raw device pointers); the library allocates
+    nothing.  Returns the library status code (0 = enqueued)."""
+    return lib().bls_verify_compressed_noalloc(sigs48_ptr, nhms_ptr, g2_ptr, pk_tables_ptr, pk_index_ptr,
+                                               results_ptr, n, lanes, stream)
+
 
 class Context:
     """A device context: stream, buffers and resident public-key tables."""

@@ -187,6 +187,27 @@ typedef struct {
 int bls_autotune(bls_ctx* ctx, const bls_batch* sample_device, int repeats, bls_tune_point* points,
                  int max_points, int* n_points);
 
+/* ---- verification without device allocation ----
+ * No counterpart in the reference: its wrapper allocates and frees device
+ * memory on every call (gpu-crypto/cuda/api.cu:137-159).  For callers that
+ * cannot call cudaMalloc while they verify -- code inside a CUDA stream
+ * capture, plugins whose host hands all device memory to its own allocator,
+ * latency-critical paths that cannot afford cudaMalloc's device-wide
+ * synchronisation.  Every pointer is device memory owned by the caller:
+ * sigs48 (n x 48 B), neg_hms (n x 12 u64), g2_coeffs (2448 u64), pk_tables
+ * (k x 2448 u64), pk_index (n), results (n, as bls_verify_batch).  The work is
+ * enqueued on `stream` (a cudaStream_t) and not synchronised.  Scratch lives
+ * in a fixed device array inside the library (about 0.8 MB on each GPU that
+ * loads it, held until exit), so at most BLS_NOALLOC_MAX_ITEMS items per call
+ * (more returns BLS_ERR_INVALID).  All calls on a device share that array:
+ * calls whose work overlaps on the GPU race and must be ordered by the
+ * caller.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  lanes_per_pairing: 2, 4 or 8. */
+#define BLS_NOALLOC_MAX_ITEMS 8192
+int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64_t* neg_hms, const uint64_t* g2_coeffs,
+                                  const uint64_t* pk_tables, const int32_t* pk_index, int32_t* results, int n,
+                                  int lanes_per_pairing, void* stream);
+
 /* Decode n compressed G1 points: status[i] (BLS_ST_*), xy[i] 12 x uint64
  * (identity: x = 0, y = R mod p; failures: zeros). */
 int bls_g1_decompress_status(bls_ctx* ctx, const uint8_t* compressed, int n, uint64_t* xy, int32_t* status);
