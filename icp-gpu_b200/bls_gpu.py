@@ -58,6 +58,11 @@ class TunePoint(ctypes.Structure):
 MODE_PLAIN, MODE_PERSISTENT = 0, 1
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("sig_format", ctypes.c_int), ("slots", ctypes.c_int), ("max_batch_items", ctypes.c_int),
+                ("mem_cap_bytes", ctypes.c_size_t)]
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("sig_format", ctypes.c_int), ("sigs", ctypes.c_void_p),
                 ("neg_hms", ctypes.c_void_p), ("pk_ids", ctypes.c_void_p),
@@ -99,6 +104,13 @@ def lib():
         L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
         L.bls_verify_compressed_noalloc.argtypes = [P, P, P, P, P, P, I, I, P]
+        L.bls_server_create.argtypes = [P, ctypes.POINTER(ServerConfig), ctypes.POINTER(P)]
+        L.bls_server_destroy.argtypes = [P]
+        L.bls_server_destroy.restype = None
+        L.bls_server_submit.argtypes = [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64),
+                                        ctypes.POINTER(ctypes.c_int64)]
+        L.bls_server_wait.argtypes = [P, ctypes.c_uint64, I, ctypes.POINTER(ctypes.c_int64)]
+        L.bls_server_stats.argtypes = [P] + [ctypes.POINTER(ctypes.c_uint64)] * 3
         L.bls_autotune.argtypes = [P, ctypes.POINTER(Batch), I, ctypes.POINTER(TunePoint), I, ctypes.POINTER(I)]
         _lib = L
     return _lib
@@ -309,3 +321,57 @@ class Context:
         self._check(self.lib.bls_autotune(self.h, ctypes.byref(b), repeats, pts, 32, ctypes.byref(npts)),
                     "bls_autotune")
         return [(pts[i].lanes_per_pairing, pts[i].blocks_per_sm, pts[i].ms) for i in range(npts.value)]
+
+
+class Server:
+    """Continuous-batching verify server on a Context (bls_server_*)."""
+
+    def __init__(self, ctx, compressed=False, slots=0, max_batch_items=0, mem_cap_bytes=0):
+        cfg = ServerConfig(SIG_COMPRESSED if compressed else SIG_AFFINE, slots, max_batch_items, mem_cap_bytes)
+        h = ctypes.c_void_p()
+        rc = ctx.lib.bls_server_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h))
+        if rc != BLS_OK:
+            raise GpuError("bls_server_create failed (%d)" % rc)
+        self.h, self.lib, self.compressed = h, ctx.lib, compressed
+        self._keep = {}
+
+    def submit(self, sigs, nhms, ids):
+        """Queue a request; returns (ticket, submit_ns, results array filled on completion)."""
+        nhms = _u64(nhms, 12)
+        n = nhms.shape[0]
+        s = np.ascontiguousarray(sigs, dtype=np.uint8).reshape(-1) if self.compressed else _u64(sigs, 12)
+        ids = np.ascontiguousarray(ids, dtype=np.int32).reshape(-1)
+        res = np.zeros(n, dtype=np.int32)
+        req = Request(n, _ptr(s), _ptr(nhms), _ptr(ids), _ptr(res))
+        t = ctypes.c_uint64()
+        ns = ctypes.c_int64()
+        rc = self.lib.bls_server_submit(self.h, ctypes.byref(req), ctypes.byref(t), ctypes.byref(ns))
+        if rc != BLS_OK:
+            raise GpuError("bls_server_submit failed (%d)" % rc)
+        self._keep[t.value] = res
+        return t.value, ns.value, res
+
+    def wait(self, ticket, timeout_ms=-1):
+        """Block until the ticket completes; returns its completion time (ns)."""
+        ns = ctypes.c_int64()
+        rc = self.lib.bls_server_wait(self.h, ticket, timeout_ms, ctypes.byref(ns))
+        if rc != BLS_OK:
+            raise GpuError("bls_server_wait failed (%d)" % rc)
+        self._keep.pop(ticket, None)
+        return ns.value
+
+    def stats(self):
+        v = [ctypes.c_uint64() for _ in range(3)]
+        self.lib.bls_server_stats(self.h, *[ctypes.byref(x) for x in v])
+        return {"launches": v[0].value, "items": v[1].value, "max_batch": v[2].value}
+
+    def close(self):
+        if self.h:
+            self.lib.bls_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

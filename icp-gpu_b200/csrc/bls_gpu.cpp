@@ -275,6 +275,14 @@ int check_ids(bls_ctx* c, const int32_t* ids, int n) {
 
 }  // namespace
 
+namespace bls {
+CtxView ctx_view(bls_ctx* c) {
+    std::lock_guard<std::mutex> lk(c->mu);
+    return CtxView{c->cfg.device, c->sms, c->cfg.lanes_per_pairing, c->cfg.blocks_per_sm,
+                   c->d_g2, c->d_pk, c->d_pk_inf, c->n_pks};
+}
+}  // namespace bls
+
 extern "C" {
 
 void bls_config_default(bls_config* cfg, int device) {

@@ -34,4 +34,13 @@ size_t verify_lanes_smem_bytes(int lanes);
 // blocks of the lane-parallel kernel resident per SM (occupancy calculator)
 int verify_lanes_blocks_per_sm(int lanes);
 
+// what the serving loop (server.cpp) needs from a context
+struct CtxView {
+    int device, sms, lanes, blocks_per_sm;
+    const uint64_t* g2;
+    const uint64_t* pk_tables;
+    const uint8_t* pk_identity;
+    int n_pks;
+};
+
 }  // namespace bls

@@ -1,0 +1,304 @@
+// Serving loop: continuous batching of verify requests (include/bls_gpu.h,
+// bls_server_*).
+//
+// The reference has no serving path: its IC integration collects shares into
+// a thread-local batch and flushes it synchronously on the caller's thread
+// (ic-integration/patches/ic-gpu-consensus.patch:286-403).  Here requests from
+// any thread go into one queue; a dispatcher thread keeps `slots` launches in
+// flight.  When a slot is free it takes every queued request that fits the
+// slot (FIFO, up to max_batch_items), copies them into the slot's pinned
+// buffers, and enqueues copy-in, the persistent verify (items claimed from the
+// slot's device counter) and copy-out on the slot's stream.  Finished slots are
+// found with cudaEventQuery; their results are copied into the requests'
+// result buffers and the tickets are released.  A request arriving while the
+// GPU works on earlier ones is admitted into the next free slot, so batches
+// overlap on the device instead of waiting for each other.
+//
+// Admission: each slot's device buffers are sized for max_batch_items and
+// counted against mem_cap_bytes at creation; the number of slots is reduced
+// to what the budget admits.  Waits are bounded (timeouts), the dispatcher
+// never spins on the device: it sleeps on a condition variable between polls.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/bls_gpu.h"
+#include "internal.h"
+
+namespace bls {
+CtxView ctx_view(bls_ctx* c);
+}
+
+namespace {
+
+int64_t now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct Pending {
+    uint64_t ticket;
+    int n;
+    std::vector<uint8_t> sigs;
+    std::vector<uint64_t> nhms;
+    std::vector<int32_t> ids;
+    int32_t* results;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    void *h_sigs = nullptr, *h_nhms = nullptr, *h_ids = nullptr, *h_res = nullptr;
+    void *d_sigs = nullptr, *d_nhms = nullptr, *d_ids = nullptr, *d_res = nullptr, *d_xy = nullptr,
+         *d_st = nullptr, *d_work = nullptr;
+    bool busy = false;
+    std::vector<Pending> reqs;
+};
+
+}  // namespace
+
+struct bls_server {
+    bls_ctx* ctx = nullptr;
+    bls_server_config cfg{};
+    bls::CtxView view{};
+    std::vector<Slot> slots;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Pending> queue;
+    std::unordered_map<uint64_t, int64_t> done;  // ticket -> completion time
+    std::atomic<bool> stop{false};
+    std::thread worker;
+    uint64_t next_ticket = 1;
+    uint64_t launches = 0, items = 0, max_batch = 0;
+    int error = 0;
+
+    size_t sig_bytes() const { return cfg.sig_format == BLS_SIG_COMPRESSED ? 48 : 96; }
+
+    int launch(Slot& s) {
+        size_t n = 0, sb = sig_bytes();
+        for (auto& r : s.reqs) {
+            memcpy((char*)s.h_sigs + n * sb, r.sigs.data(), r.n * sb);
+            memcpy((char*)s.h_nhms + n * 96, r.nhms.data(), r.n * 96);
+            memcpy((char*)s.h_ids + n * 4, r.ids.data(), r.n * 4);
+            n += r.n;
+        }
+        cudaStream_t st = s.stream;
+        if (cudaMemcpyAsync(s.d_sigs, s.h_sigs, n * sb, cudaMemcpyHostToDevice, st) ||
+            cudaMemcpyAsync(s.d_nhms, s.h_nhms, n * 96, cudaMemcpyHostToDevice, st) ||
+            cudaMemcpyAsync(s.d_ids, s.h_ids, n * 4, cudaMemcpyHostToDevice, st) ||
+            cudaMemsetAsync(s.d_work, 0, sizeof(int), st))
+            return BLS_ERR_CUDA;
+        bls::VerifyArgs a{};
+        a.sigs = s.d_sigs;
+        a.sig_compressed = cfg.sig_format == BLS_SIG_COMPRESSED;
+        a.nhms = (const uint64_t*)s.d_nhms;
+        a.g2 = view.g2;
+        a.pk_tables = view.pk_tables;
+        a.pk_index = (const int32_t*)s.d_ids;
+        a.pk_identity = view.pk_identity;
+        a.n = (int)n;
+        a.results = (int32_t*)s.d_res;
+        a.work_counter = (int*)s.d_work;
+        const uint32_t* status = nullptr;
+        if (a.sig_compressed) {
+            if (bls::launch_g1_decompress((const uint8_t*)s.d_sigs, a.n, (uint64_t*)s.d_xy, (int32_t*)s.d_st, st))
+                return BLS_ERR_CUDA;
+            a.sig_xy = (const uint64_t*)s.d_xy;
+            status = (const uint32_t*)s.d_st;
+        }
+        int lanes = view.lanes > 1 ? view.lanes : 8;
+        if (bls::launch_verify_lanes(a, status, lanes, view.blocks_per_sm, view.sms, st) ||
+            cudaMemcpyAsync(s.h_res, s.d_res, n * 4, cudaMemcpyDeviceToHost, st) || cudaEventRecord(s.done, st))
+            return BLS_ERR_CUDA;
+        s.busy = true;
+        ++launches;
+        if (n > max_batch) max_batch = n;
+        return BLS_OK;
+    }
+
+    void finish(Slot& s) {
+        size_t off = 0;
+        int64_t t = now_ns();
+        for (auto& r : s.reqs) {
+            memcpy(r.results, (const char*)s.h_res + off * 4, (size_t)r.n * 4);
+            off += r.n;
+            done[r.ticket] = t;
+        }
+        items += off;
+        s.reqs.clear();
+        s.busy = false;
+    }
+
+    void run() {
+        if (cudaSetDevice(view.device) != cudaSuccess) {
+            std::lock_guard<std::mutex> lk(mu);
+            error = BLS_ERR_CUDA;
+            cv_done.notify_all();
+            return;
+        }
+        std::unique_lock<std::mutex> lk(mu);
+        while (true) {
+            bool any_busy = false, progressed = false;
+            for (auto& s : slots) {
+                if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
+                    finish(s);
+                    progressed = true;
+                }
+                any_busy = any_busy || s.busy;
+            }
+            if (progressed) cv_done.notify_all();
+            for (auto& s : slots) {
+                if (s.busy || queue.empty()) continue;
+                size_t n = 0;
+                while (!queue.empty() && n + (size_t)queue.front().n <= (size_t)cfg.max_batch_items) {
+                    n += queue.front().n;
+                    s.reqs.push_back(std::move(queue.front()));
+                    queue.pop_front();
+                }
+                if (s.reqs.empty()) continue;
+                int rc = launch(s);
+                if (rc) {
+                    error = rc;
+                    cv_done.notify_all();
+                    return;
+                }
+                any_busy = true;
+            }
+            if (stop && queue.empty() && !any_busy) return;
+            // sleep until new work arrives or a short poll interval passes
+            cv_work.wait_for(lk, std::chrono::microseconds(any_busy ? 50 : 2000));
+        }
+    }
+};
+
+extern "C" {
+
+int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** out) {
+    if (!ctx || !out) return BLS_ERR_INVALID;
+    *out = nullptr;
+    auto* s = new bls_server();
+    s->ctx = ctx;
+    if (cfg) s->cfg = *cfg;
+    if (s->cfg.slots <= 0) s->cfg.slots = 3;
+    if (s->cfg.max_batch_items <= 0) s->cfg.max_batch_items = 16384;
+    if (s->cfg.mem_cap_bytes == 0) s->cfg.mem_cap_bytes = (size_t)4 << 30;
+    if (s->cfg.sig_format != BLS_SIG_AFFINE && s->cfg.sig_format != BLS_SIG_COMPRESSED) {
+        delete s;
+        return BLS_ERR_INVALID;
+    }
+    s->view = bls::ctx_view(ctx);
+    if (cudaSetDevice(s->view.device) != cudaSuccess) {
+        delete s;
+        return BLS_ERR_CUDA;
+    }
+    size_t m = (size_t)s->cfg.max_batch_items;
+    size_t per_slot = m * (s->sig_bytes() + 96 + 4 + 4 + 96 + 4) + 256;
+    int admitted = (int)(s->cfg.mem_cap_bytes / per_slot);
+    if (admitted < 1) {
+        delete s;
+        return BLS_ERR_NOMEM;
+    }
+    if (s->cfg.slots > admitted) s->cfg.slots = admitted;
+    s->slots.resize(s->cfg.slots);
+    for (auto& sl : s->slots) {
+        bool ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaHostAlloc(&sl.h_sigs, m * s->sig_bytes(), 0) == cudaSuccess &&
+                  cudaHostAlloc(&sl.h_nhms, m * 96, 0) == cudaSuccess && cudaHostAlloc(&sl.h_ids, m * 4, 0) == cudaSuccess &&
+                  cudaHostAlloc(&sl.h_res, m * 4, 0) == cudaSuccess && cudaMalloc(&sl.d_sigs, m * s->sig_bytes()) == cudaSuccess &&
+                  cudaMalloc(&sl.d_nhms, m * 96) == cudaSuccess && cudaMalloc(&sl.d_ids, m * 4) == cudaSuccess &&
+                  cudaMalloc(&sl.d_res, m * 4) == cudaSuccess && cudaMalloc(&sl.d_xy, m * 96) == cudaSuccess &&
+                  cudaMalloc(&sl.d_st, m * 4) == cudaSuccess && cudaMalloc(&sl.d_work, 256) == cudaSuccess;
+        if (!ok) {
+            bls_server_destroy(s);
+            return BLS_ERR_NOMEM;
+        }
+    }
+    // set up the kernel (shared-memory size, occupancy) before serving
+    bls::verify_lanes_blocks_per_sm(s->view.lanes > 1 ? s->view.lanes : 8);
+    s->worker = std::thread([s] { s->run(); });
+    *out = s;
+    return BLS_OK;
+}
+
+void bls_server_destroy(bls_server* s) {
+    if (!s) return;
+    if (s->worker.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stop = true;
+        }
+        s->cv_work.notify_all();
+        s->worker.join();
+    }
+    cudaSetDevice(s->view.device);
+    for (auto& sl : s->slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        for (void* p : {sl.h_sigs, sl.h_nhms, sl.h_ids, sl.h_res})
+            if (p) cudaFreeHost(p);
+        for (void* p : {sl.d_sigs, sl.d_nhms, sl.d_ids, sl.d_res, sl.d_xy, sl.d_st, sl.d_work})
+            if (p) cudaFree(p);
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    delete s;
+}
+
+int bls_server_submit(bls_server* s, const bls_request* r, uint64_t* ticket, int64_t* submit_ns) {
+    if (!s || !r || !ticket) return BLS_ERR_INVALID;
+    if (r->n <= 0 || r->n > s->cfg.max_batch_items) return BLS_ERR_INVALID;
+    if (!r->sigs || !r->neg_hms || !r->pk_ids || !r->results) return BLS_ERR_INVALID;
+    for (int i = 0; i < r->n; ++i)
+        if (r->pk_ids[i] < 0 || r->pk_ids[i] >= s->view.n_pks) return BLS_ERR_INVALID;
+    Pending p;
+    p.n = r->n;
+    p.sigs.assign((const uint8_t*)r->sigs, (const uint8_t*)r->sigs + (size_t)r->n * s->sig_bytes());
+    p.nhms.assign(r->neg_hms, r->neg_hms + (size_t)r->n * 12);
+    p.ids.assign(r->pk_ids, r->pk_ids + r->n);
+    p.results = r->results;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->error) return s->error;
+        p.ticket = s->next_ticket++;
+        *ticket = p.ticket;
+        if (submit_ns) *submit_ns = now_ns();
+        s->queue.push_back(std::move(p));
+    }
+    s->cv_work.notify_one();
+    return BLS_OK;
+}
+
+int bls_server_wait(bls_server* s, uint64_t ticket, int timeout_ms, int64_t* done_ns) {
+    if (!s) return BLS_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto ready = [&] { return s->error != 0 || s->done.count(ticket) != 0; };
+    if (timeout_ms < 0) {
+        s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+        return BLS_ERR_TIMEOUT;
+    }
+    if (s->error) return s->error;
+    auto it = s->done.find(ticket);
+    if (done_ns) *done_ns = it->second;
+    s->done.erase(it);
+    return BLS_OK;
+}
+
+int bls_server_stats(bls_server* s, uint64_t* launches, uint64_t* items, uint64_t* max_batch) {
+    if (!s) return BLS_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (launches) *launches = s->launches;
+    if (items) *items = s->items;
+    if (max_batch) *max_batch = s->max_batch;
+    return BLS_OK;
+}
+
+}  // extern "C"

@@ -198,7 +198,7 @@ def _items(rng, keys, key_of_item, corrupt):
 
 
 def config_plain(n=64, seed=1):
-    """n keys, one signature each, every 8th message bit-flipped."""
+    """Plain workload: n keys, one signature each, every 8th message bit-flipped."""
     rng = SplitMix64(seed)
     keys = _keys(rng, n)
     corrupt = [1 if i % 8 == 7 else 0 for i in range(n)]
@@ -212,7 +212,7 @@ def _split_corruption(n):
 
 
 def config_keyset(n=4096, nkeys=40, seed=2):
-    """n verifications over nkeys resident keys (key i % nkeys)."""
+    """Key-set workload: n verifications over nkeys resident keys (key i % nkeys)."""
     rng = SplitMix64(seed)
     keys = _keys(rng, nkeys)
     it = _items(rng, keys, [i % nkeys for i in range(n)], _split_corruption(n))
@@ -220,7 +220,7 @@ def config_keyset(n=4096, nkeys=40, seed=2):
 
 
 def config_compressed(n=65536, nkeys=40, seed=3, invalid_frac=0.02):
-    """n compressed signatures; invalid_frac of them are invalid
+    """Compressed workload: n compressed signatures; invalid_frac of them are invalid
     encodings, the reason per index known: bad flags (three kinds), x >= p, x
     off the curve, a curve point outside the subgroup."""
     rng = SplitMix64(seed)
@@ -281,7 +281,7 @@ def loguniform_sizes(rng, count, hi):
 
 
 def config_requests(nreq=256, max_size=2048, nkeys=40, seed=4):
-    """nreq requests of log-uniform size in [1, max_size], each over
+    """Batching workload: nreq requests of log-uniform size in [1, max_size], each over
     1..nkeys keys drawn from the pool.  Items are concatenated; offsets[r] is
     the first item of request r."""
     rng = SplitMix64(seed)
@@ -301,7 +301,7 @@ def config_requests(nreq=256, max_size=2048, nkeys=40, seed=4):
 
 
 def config_pool(n=8192, nkeys=40, seed=5):
-    """Item pool the serving stream (configs[4]) draws its requests from."""
+    """Item pool the serving stream draws its requests from."""
     rng = SplitMix64(seed)
     keys = _keys(rng, nkeys)
     it = _items(rng, keys, [i % nkeys for i in range(n)], _split_corruption(n))

@@ -187,6 +187,35 @@ typedef struct {
 int bls_autotune(bls_ctx* ctx, const bls_batch* sample_device, int repeats, bls_tune_point* points,
                  int max_points, int* n_points);
 
+/* ---- serving: continuous batching of arriving requests ----
+ * A server owns a dispatcher thread and `slots` launch slots (each a stream
+ * with its own pinned and device buffers).  Submitted requests queue; when a
+ * slot is free the dispatcher takes every queued request that fits the slot's
+ * item capacity, stages them and launches them as one persistent verify on the
+ * slot's stream, so batches formed while others run overlap on the device.
+ * Device memory for the slots is admitted against mem_cap_bytes. */
+typedef struct bls_server bls_server;
+
+typedef struct {
+    int sig_format;            /* of every request submitted */
+    int slots;                 /* launches in flight (0 = 3) */
+    int max_batch_items;       /* items per launch (0 = 16384) */
+    size_t mem_cap_bytes;      /* device memory for the slots (0 = 4 GiB) */
+} bls_server_config;
+
+int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** out);
+/* waits for in-flight work, then frees the server */
+void bls_server_destroy(bls_server* srv);
+/* Queue one request (inputs are copied; results are written to req->results
+ * when it completes).  *ticket identifies it; *submit_ns is the submit time
+ * (steady clock).  Requests larger than max_batch_items are rejected. */
+int bls_server_submit(bls_server* srv, const bls_request* req, uint64_t* ticket, int64_t* submit_ns);
+/* Wait up to timeout_ms (negative: forever) for a ticket; *done_ns is its
+ * completion time.  BLS_ERR_TIMEOUT when it has not completed. */
+int bls_server_wait(bls_server* srv, uint64_t ticket, int timeout_ms, int64_t* done_ns);
+/* counters: launches, items completed, largest batch */
+int bls_server_stats(bls_server* srv, uint64_t* launches, uint64_t* items, uint64_t* max_batch);
+
 /* ---- verification without device allocation ----
  * No counterpart in the reference: its wrapper allocates and frees device
  * memory on every call (gpu-crypto/cuda/api.cu:137-159).  For callers that

@@ -1,0 +1,99 @@
+"""GPU tests of the serving loop (bls_server_*): requests submitted from
+several threads while others are on the device are batched together, and each
+request's results are identical to verifying it alone and to the expected
+accept bits (exact integer results: the tolerance is zero)."""
+import threading
+
+import numpy as np
+import pytest
+
+import bls_gpu as G
+import workload as WL
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pool():
+    return WL.config_pool(n=1024, nkeys=40, seed=5)
+
+
+def _ids(ctx, pool):
+    return np.array([ctx.register_pk_affine(q) for q in pool["pk_affine"]], dtype=np.int32)
+
+
+def _requests(pool, nreq, max_size, seed):
+    rng = np.random.default_rng(seed)
+    n = len(pool["expect"])
+    out = []
+    for _ in range(nreq):
+        s = int(min(max_size, max(1, np.exp(rng.uniform() * np.log(max_size + 1)))))
+        idx = (int(rng.integers(n)) + np.arange(s)) % n
+        out.append(idx)
+    return out
+
+
+def test_mix_equals_alone_and_expected(pool):
+    with G.Context() as ctx:
+        ids = _ids(ctx, pool)
+        pk_ids = ids[pool["pk_index"]]
+        reqs = _requests(pool, 60, 200, seed=1)
+        alone = [ctx.verify(pool["sigs"][ix], pool["nhms"][ix], pk_ids[ix]) for ix in reqs]
+        with G.Server(ctx, slots=3, max_batch_items=512) as srv:
+            tickets = [None] * len(reqs)
+
+            def submit(k0):
+                for k in range(k0, len(reqs), 3):
+                    ix = reqs[k]
+                    tickets[k] = srv.submit(pool["sigs"][ix], pool["nhms"][ix], pk_ids[ix])
+
+            th = [threading.Thread(target=submit, args=(k,)) for k in range(3)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            for k, (ticket, t_sub, res) in enumerate(tickets):
+                t_done = srv.wait(ticket, timeout_ms=60000)
+                assert t_done >= t_sub
+                assert (res == alone[k]).all()
+                assert (res == pool["expect"][reqs[k]]).all()
+            st = srv.stats()
+        assert st["items"] == sum(len(ix) for ix in reqs)
+        # requests arriving together were batched: fewer launches than requests
+        assert 1 <= st["launches"] < len(reqs)
+        assert st["max_batch"] <= 512
+
+
+def test_compressed_stream_with_invalid():
+    cc = WL.config_compressed(256, 40, seed=9, invalid_frac=0.05)
+    with G.Context() as ctx:
+        ids = np.array([ctx.register_pk_affine(q) for q in cc["pk_affine"]], dtype=np.int32)
+        pk_ids = ids[cc["pk_index"]]
+        cuts = [0, 1, 40, 41, 130, 256]
+        with G.Server(ctx, compressed=True, slots=2, max_batch_items=128) as srv:
+            tk = []
+            for a, b in zip(cuts, cuts[1:]):
+                tk.append((a, b, srv.submit(cc["sigs_compressed"][a:b], cc["nhms"][a:b], pk_ids[a:b])))
+            for a, b, (ticket, _, res) in tk:
+                srv.wait(ticket, timeout_ms=60000)
+                assert (res == cc["expect"][a:b]).all()
+
+
+def test_admission_and_argument_errors(pool):
+    with G.Context() as ctx:
+        ids = _ids(ctx, pool)
+        # a budget too small for one slot is refused
+        with pytest.raises(G.GpuError):
+            G.Server(ctx, max_batch_items=4096, mem_cap_bytes=1 << 16)
+        with G.Server(ctx, slots=8, max_batch_items=64, mem_cap_bytes=64 * 400 * 2 + 1024) as srv:
+            bad = np.full(3, 999, dtype=np.int32)
+            with pytest.raises(G.GpuError):
+                srv.submit(pool["sigs"][:3], pool["nhms"][:3], bad)
+            with pytest.raises(G.GpuError):   # larger than a slot
+                n = 65
+                srv.submit(pool["sigs"][:n], pool["nhms"][:n], ids[pool["pk_index"][:n]])
+            t, _, res = srv.submit(pool["sigs"][:5], pool["nhms"][:5], ids[pool["pk_index"][:5]])
+            srv.wait(t, timeout_ms=60000)
+            assert (res == pool["expect"][:5]).all()
+            with pytest.raises(G.GpuError):   # unknown ticket: times out
+                srv.wait(t + 1000, timeout_ms=10)

@@ -15,7 +15,7 @@ def g2_affine_u64(q):
 
 
 def plain_config(n=64, seed=1):
-    """configs[0] from the workload generator, plus the signatures as oracle
+    """The plain workload from the workload generator, plus the signatures as oracle
     points (for encoding tests)."""
     c = WL.config_plain(n, seed)
     return {
