@@ -313,7 +313,8 @@ def run_gpu(args):
                           % (sms, clk),
             "algorithmic_imad_per_verify": ALGO_IMAD_PER_VERIFY,
             "own_imad_per_verify": IMAD_PER_VERIFY, "own_fp_muls_per_verify": FP_MULS_PER_VERIFY,
-            "kernel": "k_verify_lanes<%d>" % args.lanes if args.lanes > 1 else "k_verify",
+            "kernel": ("k_verify_fp2" if args.lanes == 6 else "k_verify_lanes<%d>" % args.lanes) if args.lanes > 1
+            else "k_verify",
             "kernel_ms": round(kernel_ms, 4),
         }
         result = {
@@ -456,7 +457,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batching and serving sections")
-    ap.add_argument("--lanes", type=int, default=8, help="lanes per verification (1, 2, 4, 8)")
+    ap.add_argument("--lanes", type=int, default=6, help="lanes per verification (6: Fp2-lane kernel; 1, 2, 4, 8)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the serving stream (0 = skip)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -146,10 +146,10 @@ int ctx_init(bls_ctx* c, const bls_config* cfg) {
     c->cfg = *cfg;
     if (c->cfg.max_batch <= 0) c->cfg.max_batch = 65536;
     if (c->cfg.max_pks <= 0) c->cfg.max_pks = 1024;
-    if (c->cfg.lanes_per_pairing <= 0) c->cfg.lanes_per_pairing = 8;
+    if (c->cfg.lanes_per_pairing <= 0) c->cfg.lanes_per_pairing = 6;
     int l = c->cfg.lanes_per_pairing;
-    if (l != 1 && l != 2 && l != 4 && l != 8)
-        return fail(BLS_ERR_INVALID, "lanes_per_pairing must be 1, 2, 4 or 8 (got %d)", l);
+    if (l != 1 && l != 2 && l != 4 && l != 6 && l != 8)
+        return fail(BLS_ERR_INVALID, "lanes_per_pairing must be 1, 2, 4, 6 or 8 (got %d)", l);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return fail(BLS_ERR_NODEV, "no CUDA device");
@@ -494,7 +494,7 @@ int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* 
     struct Cand { int lanes, bps; };
     std::vector<Cand> cands;
     cands.push_back({1, 0});
-    for (int l : {2, 4, 8}) {
+    for (int l : {2, 4, 6, 8}) {
         int res = bls::verify_lanes_blocks_per_sm(l);
         cands.push_back({l, 0});
         for (int bps : {res - 1, res / 2})

@@ -1,0 +1,340 @@
+// Device arithmetic of the Fp2-lane verify kernel (verify_fp2.cu): products
+// into double-width accumulators, one Montgomery reduction per output, and
+// the QP reduction that keeps every slot below 2^381 + p.  The generator's
+// emulator (gen_fp2ops.py) models each routine here bit for bit.
+#pragma once
+#include "fp.cuh"
+#include "fp2ops.inc"
+
+namespace bls {
+namespace f2 {
+
+// p[0..23] = a * b, schoolbook rows with the CIOS carry chains of fp.cuh.
+// After row i the partial product is below 2^(384 + 32 (i + 1)), so the hi
+// chain never carries out of p[i + 12].
+__device__ __forceinline__ void prod24(uint32_t* p, const uint32_t* a, const uint32_t* b) {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) p[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        chain_lo(p + i, a, b[i]);
+        chain_hi(p + i, a, b[i]);
+    }
+}
+
+// acc[0..25] += coef * p (coef in {-4, -2, -1, 0, 1, 2, 4}), modulo 2^832.
+// The operand is (p << s) masked to zero for coef == 0 and complemented for a
+// negative coef, with the complement's +1 entering as the first carry.
+__device__ __forceinline__ void acc_add(uint32_t* acc, const uint32_t* p, int coef) {
+    const int mag = coef < 0 ? -coef : coef;
+    const uint32_t s = mag >> 1;                    // 1 -> 0, 2 -> 1, 4 -> 2
+    const uint32_t z = coef != 0 ? 0xffffffffu : 0u;
+    const uint32_t m = coef < 0 ? 0xffffffffu : 0u;
+    uint32_t v[26];
+    v[0] = ((p[0] << s) & z) ^ m;
+#pragma unroll
+    for (int i = 1; i < 24; ++i) v[i] = (__funnelshift_l(p[i - 1], p[i], s) & z) ^ m;
+    v[24] = (__funnelshift_l(p[23], 0u, s) & z) ^ m;
+    v[25] = m;
+    const uint32_t cin = m & 1u;
+    uint32_t dummy;
+    asm("add.cc.u32 %26, %27, 0xffffffff;\n\t"
+        "addc.cc.u32 %0, %0, %28;\n\t"
+        "addc.cc.u32 %1, %1, %29;\n\t"
+        "addc.cc.u32 %2, %2, %30;\n\t"
+        "addc.cc.u32 %3, %3, %31;\n\t"
+        "addc.cc.u32 %4, %4, %32;\n\t"
+        "addc.cc.u32 %5, %5, %33;\n\t"
+        "addc.cc.u32 %6, %6, %34;\n\t"
+        "addc.cc.u32 %7, %7, %35;\n\t"
+        "addc.cc.u32 %8, %8, %36;\n\t"
+        "addc.cc.u32 %9, %9, %37;\n\t"
+        "addc.cc.u32 %10, %10, %38;\n\t"
+        "addc.cc.u32 %11, %11, %39;\n\t"
+        "addc.cc.u32 %12, %12, %40;\n\t"
+        "addc.cc.u32 %13, %13, %41;\n\t"
+        "addc.cc.u32 %14, %14, %42;\n\t"
+        "addc.cc.u32 %15, %15, %43;\n\t"
+        "addc.cc.u32 %16, %16, %44;\n\t"
+        "addc.cc.u32 %17, %17, %45;\n\t"
+        "addc.cc.u32 %18, %18, %46;\n\t"
+        "addc.cc.u32 %19, %19, %47;\n\t"
+        "addc.cc.u32 %20, %20, %48;\n\t"
+        "addc.cc.u32 %21, %21, %49;\n\t"
+        "addc.cc.u32 %22, %22, %50;\n\t"
+        "addc.cc.u32 %23, %23, %51;\n\t"
+        "addc.cc.u32 %24, %24, %52;\n\t"
+        "addc.u32 %25, %25, %53;"
+        : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3]), "+r"(acc[4]), "+r"(acc[5]), "+r"(acc[6]),
+          "+r"(acc[7]), "+r"(acc[8]), "+r"(acc[9]), "+r"(acc[10]), "+r"(acc[11]), "+r"(acc[12]), "+r"(acc[13]),
+          "+r"(acc[14]), "+r"(acc[15]), "+r"(acc[16]), "+r"(acc[17]), "+r"(acc[18]), "+r"(acc[19]),
+          "+r"(acc[20]), "+r"(acc[21]), "+r"(acc[22]), "+r"(acc[23]), "+r"(acc[24]), "+r"(acc[25]), "=r"(dummy)
+        : "r"(cin), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+          "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]),
+          "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]),
+          "r"(v[24]), "r"(v[25]));
+}
+
+// t[0..12] = k * p for a small k (k < 2^32)
+__device__ __forceinline__ void set_kp(uint32_t* t, uint32_t k) {
+#pragma unroll
+    for (int i = 0; i < 13; ++i) t[i] = 0;
+    chain_lo_p(t, k);
+    chain_hi_p(t, k);
+}
+
+// Montgomery reduction of a 26-limb accumulator (value below 2^771):
+// r[0..12] = acc / 2^384 mod p, as acc_hi + (acc_lo + M p) / 2^384 (below 2^388).
+// The low half is reduced with the CIOS rows of fp.cuh: 12 rows of
+// m = t0 * (-p^-1), t += m p, shift, on a 13-limb window.
+__device__ __forceinline__ void redc26(uint32_t* r, const uint32_t* acc) {
+    uint32_t t[13];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) t[i] = acc[i];
+    t[12] = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        uint32_t m = t[0] * BLS_NINV;
+        chain_lo_p(t, m);
+        chain_hi_p(t, m);
+#pragma unroll
+        for (int j = 0; j < 12; ++j) t[j] = t[j + 1];
+        t[12] = 0;
+    }
+    asm("add.cc.u32 %0, %13, %26;\n\t"
+        "addc.cc.u32 %1, %14, %27;\n\t"
+        "addc.cc.u32 %2, %15, %28;\n\t"
+        "addc.cc.u32 %3, %16, %29;\n\t"
+        "addc.cc.u32 %4, %17, %30;\n\t"
+        "addc.cc.u32 %5, %18, %31;\n\t"
+        "addc.cc.u32 %6, %19, %32;\n\t"
+        "addc.cc.u32 %7, %20, %33;\n\t"
+        "addc.cc.u32 %8, %21, %34;\n\t"
+        "addc.cc.u32 %9, %22, %35;\n\t"
+        "addc.cc.u32 %10, %23, %36;\n\t"
+        "addc.cc.u32 %11, %24, %37;\n\t"
+        "addc.u32 %12, %25, 0;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12])
+        : "r"(acc[12]), "r"(acc[13]), "r"(acc[14]), "r"(acc[15]), "r"(acc[16]), "r"(acc[17]), "r"(acc[18]),
+          "r"(acc[19]), "r"(acc[20]), "r"(acc[21]), "r"(acc[22]), "r"(acc[23]), "r"(acc[24]),
+          "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]), "r"(t[8]),
+          "r"(t[9]), "r"(t[10]), "r"(t[11]));
+}
+
+// v (13 limbs, below 2^388) -> v - QP[v >> 381], below 2^381 + p (12 limbs)
+__device__ __forceinline__ void qp_reduce(uint32_t* out, const uint32_t* v) {
+    const uint32_t h = (v[12] << 3) | (v[11] >> 29);
+    const uint4* q = reinterpret_cast<const uint4*>(kQP2[h & 127]);
+    const uint4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+    uint32_t top;
+    asm("sub.cc.u32 %0, %13, %26;\n\t"
+        "subc.cc.u32 %1, %14, %27;\n\t"
+        "subc.cc.u32 %2, %15, %28;\n\t"
+        "subc.cc.u32 %3, %16, %29;\n\t"
+        "subc.cc.u32 %4, %17, %30;\n\t"
+        "subc.cc.u32 %5, %18, %31;\n\t"
+        "subc.cc.u32 %6, %19, %32;\n\t"
+        "subc.cc.u32 %7, %20, %33;\n\t"
+        "subc.cc.u32 %8, %21, %34;\n\t"
+        "subc.cc.u32 %9, %22, %35;\n\t"
+        "subc.cc.u32 %10, %23, %36;\n\t"
+        "subc.cc.u32 %11, %24, %37;\n\t"
+        "subc.u32 %12, %25, %38;"
+        : "=r"(out[0]), "=r"(out[1]), "=r"(out[2]), "=r"(out[3]), "=r"(out[4]), "=r"(out[5]), "=r"(out[6]),
+          "=r"(out[7]), "=r"(out[8]), "=r"(out[9]), "=r"(out[10]), "=r"(out[11]), "=r"(top)
+        : "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+          "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(q0.x), "r"(q0.y), "r"(q0.z), "r"(q0.w), "r"(q1.x),
+          "r"(q1.y), "r"(q1.z), "r"(q1.w), "r"(q2.x), "r"(q2.y), "r"(q2.z), "r"(q2.w), "r"(q3.x));
+    (void)top;  // zero: v - QP[h] < 2^384
+}
+
+// t (13 limbs) += c * x (x 12 limbs, |c| small), modulo 2^416
+__device__ __forceinline__ void madd13(uint32_t* t, const uint32_t* x, int c) {
+    if (c >= 0) {
+        chain_lo(t, x, (uint32_t)c);
+        chain_hi(t, x, (uint32_t)c);
+    } else {
+        uint32_t u[13];
+#pragma unroll
+        for (int i = 0; i < 13; ++i) u[i] = 0;
+        chain_lo(u, x, (uint32_t)(-c));
+        chain_hi(u, x, (uint32_t)(-c));
+        uint32_t b = 0;
+#pragma unroll
+        for (int i = 0; i < 13; ++i) {
+            uint64_t d = (uint64_t)t[i] - u[i] - b;
+            t[i] = (uint32_t)d;
+            b = (uint32_t)(d >> 63);
+        }
+    }
+}
+
+// r = a + b (12 limbs, no carry out: both below 2^383)
+__device__ __forceinline__ void add12(uint32_t* r, const uint32_t* a, const uint32_t* b) {
+    asm("add.cc.u32 %0, %12, %24;\n\t"
+        "addc.cc.u32 %1, %13, %25;\n\t"
+        "addc.cc.u32 %2, %14, %26;\n\t"
+        "addc.cc.u32 %3, %15, %27;\n\t"
+        "addc.cc.u32 %4, %16, %28;\n\t"
+        "addc.cc.u32 %5, %17, %29;\n\t"
+        "addc.cc.u32 %6, %18, %30;\n\t"
+        "addc.cc.u32 %7, %19, %31;\n\t"
+        "addc.cc.u32 %8, %20, %32;\n\t"
+        "addc.cc.u32 %9, %21, %33;\n\t"
+        "addc.cc.u32 %10, %22, %34;\n\t"
+        "addc.u32 %11, %23, %35;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11])
+        : BLS_A12(a), BLS_A12(b));
+}
+
+// r = a + 3p - b (12 limbs; a, b below 2^381 + p, result below 2^384)
+__device__ __forceinline__ void add3p_sub(uint32_t* r, const uint32_t* a, const uint32_t* b) {
+    uint32_t s[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) s[i] = k3P[i];
+    add12(s, s, a);
+    asm("sub.cc.u32 %0, %12, %24;\n\t"
+        "subc.cc.u32 %1, %13, %25;\n\t"
+        "subc.cc.u32 %2, %14, %26;\n\t"
+        "subc.cc.u32 %3, %15, %27;\n\t"
+        "subc.cc.u32 %4, %16, %28;\n\t"
+        "subc.cc.u32 %5, %17, %29;\n\t"
+        "subc.cc.u32 %6, %18, %30;\n\t"
+        "subc.cc.u32 %7, %19, %31;\n\t"
+        "subc.cc.u32 %8, %20, %32;\n\t"
+        "subc.cc.u32 %9, %21, %33;\n\t"
+        "subc.cc.u32 %10, %22, %34;\n\t"
+        "subc.u32 %11, %23, %35;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11])
+        : BLS_A12(s), BLS_A12(b));
+}
+
+// ---------------------------------------------------------------------------
+// Fp inverse by the binary extended Euclidean algorithm (Knuth, TAOCP vol. 2,
+// 4.5.2; Menezes et al., Handbook of Applied Cryptography, Alg. 14.61 in its
+// modular form).  Variable time: the inputs are public.  x: Montgomery form
+// of a (any value below 2^381 + p); returns a^-1 in Montgomery form (0 for 0).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool u_is_one(const uint32_t* u) {
+    uint32_t o = u[0] ^ 1u;
+#pragma unroll
+    for (int i = 1; i < 12; ++i) o |= u[i];
+    return o == 0;
+}
+__device__ __forceinline__ bool geq12(const uint32_t* a, const uint32_t* b) {
+    uint32_t d[12], br = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        uint64_t t = (uint64_t)a[i] - b[i] - br;
+        d[i] = (uint32_t)t;
+        br = (uint32_t)(t >> 63);
+    }
+    (void)d;
+    return br == 0;
+}
+__device__ __forceinline__ void sub12(uint32_t* a, const uint32_t* b) {
+    uint32_t br = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        uint64_t t = (uint64_t)a[i] - b[i] - br;
+        a[i] = (uint32_t)t;
+        br = (uint32_t)(t >> 63);
+    }
+}
+// x = x / 2 mod p for x < p
+__device__ __forceinline__ void half_mod(uint32_t* x) {
+    const uint32_t P_[12] = {BLS_P0, BLS_P1, BLS_P2, BLS_P3, BLS_P4, BLS_P5,
+                             BLS_P6, BLS_P7, BLS_P8, BLS_P9, BLS_P10, BLS_P11};
+    const uint32_t odd = 0u - (x[0] & 1u);
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        uint64_t t = (uint64_t)x[i] + (P_[i] & odd) + c;
+        x[i] = (uint32_t)t;
+        c = (uint32_t)(t >> 32);
+    }
+#pragma unroll
+    for (int i = 0; i < 11; ++i) x[i] = __funnelshift_r(x[i], x[i + 1], 1);
+    x[11] = (x[11] >> 1) | (c << 31);
+}
+__device__ __forceinline__ void shr1(uint32_t* u) {
+#pragma unroll
+    for (int i = 0; i < 11; ++i) u[i] = __funnelshift_r(u[i], u[i + 1], 1);
+    u[11] >>= 1;
+}
+// x1 = x1 - x2 mod p (both < p)
+__device__ __forceinline__ void sub_mod(uint32_t* x1, const uint32_t* x2) {
+    const uint32_t P_[12] = {BLS_P0, BLS_P1, BLS_P2, BLS_P3, BLS_P4, BLS_P5,
+                             BLS_P6, BLS_P7, BLS_P8, BLS_P9, BLS_P10, BLS_P11};
+    uint32_t br = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        uint64_t t = (uint64_t)x1[i] - x2[i] - br;
+        x1[i] = (uint32_t)t;
+        br = (uint32_t)(t >> 63);
+    }
+    const uint32_t m = 0u - br;
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        uint64_t t = (uint64_t)x1[i] + (P_[i] & m) + c;
+        x1[i] = (uint32_t)t;
+        c = (uint32_t)(t >> 32);
+    }
+}
+
+static __device__ __noinline__ fp fp_inverse_mont(fp x) {
+    // canonical representative (x < 2^381 + p < 3p)
+    uint32_t d[12];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        uint32_t br = sub_p(d, x.w);
+#pragma unroll
+        for (int i = 0; i < 12; ++i) x.w[i] = br ? x.w[i] : d[i];
+    }
+    if (fp_is_zero(x)) return x;
+    uint32_t u[12], v[12], x1[12], x2[12];
+    const uint32_t P_[12] = {BLS_P0, BLS_P1, BLS_P2, BLS_P3, BLS_P4, BLS_P5,
+                             BLS_P6, BLS_P7, BLS_P8, BLS_P9, BLS_P10, BLS_P11};
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        u[i] = x.w[i];
+        v[i] = P_[i];
+        x1[i] = 0;
+        x2[i] = 0;
+    }
+    x1[0] = 1;
+    // u, v stay odd-or-positive and gcd(u, v) = 1; every pass of the outer
+    // loop removes at least one bit from u or v, so 2 * 381 + 2 passes end it
+    for (int iter = 0; iter < 800 && !u_is_one(u) && !u_is_one(v); ++iter) {
+        for (int k = 0; k < 384 && (u[0] & 1u) == 0; ++k) {
+            shr1(u);
+            half_mod(x1);
+        }
+        for (int k = 0; k < 384 && (v[0] & 1u) == 0; ++k) {
+            shr1(v);
+            half_mod(x2);
+        }
+        if (geq12(u, v)) {
+            sub12(u, v);
+            sub_mod(x1, x2);
+        } else {
+            sub12(v, u);
+            sub_mod(x2, x1);
+        }
+    }
+    fp r;
+    const bool uone = u_is_one(u);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) r.w[i] = uone ? x1[i] : x2[i];
+    fp r3;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) r3.w[i] = kR3[i];
+    return fp_mul(r, r3);
+}
+
+}  // namespace f2
+}  // namespace bls

@@ -1,0 +1,607 @@
+"""Generator of the Fp2-lane tower programs of the verify kernel (verify_fp2.cu).
+
+Execution model.  Six lanes own one pairing; lane k produces the k-th Fp2
+coefficient (tower order c0.c0, c0.c1, c0.c2, c1.c0, c1.c1, c1.c2) of each
+Fp12 result.  Every coefficient of every tower operation on the verify path
+(gpu-crypto/cuda/field_sppark.cuh:52-197, gpu-crypto/cuda/api.cu:22-78) is
+written as one *output*:
+
+    out = post( REDC(ACC_re), REDC(ACC_im) )
+    ACC = bias + sum over terms of  alpha_j * U_j * V_j   (exact, 832-bit)
+
+so a lane multiplies all the Fp2 products that feed its coefficient into two
+double-width accumulators and performs one Montgomery reduction per Fp
+(lazy reduction, Aranha et al., "Faster explicit formulas for computing
+pairings over ordinary curves", EUROCRYPT 2011).  Karatsuba inside each Fp2
+product; no intermediate result is rounded to Fp.
+
+Term kinds (X, Y are Fp2 slots, x0/x1 their components):
+  KARA   X*Y          U = (x0, x1, x0+x1)  V = (y0, y1, y0+y1)
+  SQR    X^2          U = (x0+x1, x0)      V = (x0-x1+3p, x1)
+  FPMUL  X*y (y in Fp) U = (x0, x1)        V = (y, y)
+  NORM   x0^2+x1^2    U = (x0, x1)         V = (x0, x1)
+with per-product accumulator coefficients (alpha for ACC_re, beta for ACC_im)
+fixed by the kind and by `xi` (multiply the term by xi = 1 + u), then scaled by
+the term's sign and doubling.  Additive multiples of p (the 3p above, the
+biases) leave every value unchanged mod p.
+
+Post-processing of an output:
+  SIMPLE  out = QP(r)                               r = REDC result
+  FULL    out = QP(c_re * QP(r_re) + sum c_j z_j + bias)  (and im with c_im)
+  LIN     out = QP(sum c_j z_j + bias)               (no product)
+  INVFP   out = (x0^-1 in Montgomery form, 0)        (one lane)
+QP(v) = v - QP[v >> 381], QP[h] = floor(h * 2^381 / p) * p: a value below
+2^388 becomes one below 2^381 + p < 2.3p; every slot holds such a value.
+
+Outputs:
+  fp2ops.inc   descriptor tables (run `python gen_fp2ops.py`)
+  Emulator     bit-exact Python model of the device arithmetic, used by the
+               tests to check every program against the oracle on the CPU.
+"""
+import os
+import sys
+
+P = 0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab
+R = 1 << 384
+NPRIME = (-pow(P, -1, 1 << 32)) % (1 << 32)
+QP = [(h << 381) // P * P for h in range(128)]
+SLOT_BOUND = (1 << 381) + P          # every slot value is below this
+ACC_LIMIT = 1 << 771                 # accumulators stay below (REDC output < 2^388)
+POST_LIMIT = 1 << 388                # QP input limit
+K3P = 3 * P
+
+# ---------------------------------------------------------------- refs
+# A ref names one Fp2 slot: base (3 bits) << 4 | index (4 bits).
+B_D, B_A, B_B, B_C, B_K, B_T = range(6)
+BASE_NAMES = "DABCKT"
+
+
+def ref(base, idx):
+    assert 0 <= idx < 16
+    return (base << 4) | idx
+
+
+# block-shared constant slots (Fp2)
+K_ZERO, K_ONE = 0, 1
+K_FROB = 2     # 2..6: conj(k1), conj(k2), conj(k12), conj(k1 k12), conj(k2 k12)
+
+# C area of a pairing: pair j (0, 1) at 6 j: coefficient c0, c1, c2, point (x, y), l2, l3
+C_C0, C_C1, C_C2, C_PT, C_L2, C_L3 = range(6)
+
+# ---------------------------------------------------------------- kinds
+KARA, SQR, FPMUL, NORM = range(4)
+# (alpha, beta) per product, plain and times xi
+COEF = {
+    (KARA, 0): ((1, -1, 0), (-1, -1, 1)),
+    (KARA, 1): ((2, 0, -1), (0, -2, 1)),
+    (SQR, 0): ((1, 0), (0, 2)),
+    (SQR, 1): ((1, -2), (1, 2)),
+    (FPMUL, 0): ((1, 0), (0, 1)),
+    (FPMUL, 1): ((1, -1), (1, 1)),
+    (NORM, 0): ((1, 1), (0, 0)),
+}
+NPROD = {KARA: 3, SQR: 2, FPMUL: 2, NORM: 2}
+M_SIMPLE, M_FULL, M_LIN, M_INVFP = range(4)
+
+
+class Term:
+    __slots__ = ("kind", "x", "y", "xi", "sign", "dbl", "yim")
+
+    def __init__(self, kind, x, y=None, xi=0, sign=1, dbl=0, yim=0):
+        self.kind, self.x, self.y, self.xi, self.sign, self.dbl, self.yim = kind, x, y, xi, sign, dbl, yim
+        if kind in (SQR, NORM):
+            self.y = x
+        assert not (kind == NORM and xi)
+
+    def coefs(self):
+        a, b = COEF[(self.kind, self.xi)]
+        m = self.sign * (2 if self.dbl else 1)
+        return [m * v for v in a], [m * v for v in b]
+
+    def operands(self, X, Y):
+        """(U, V) integer pairs for the products, from component values."""
+        x0, x1 = X
+        if self.kind == KARA:
+            y0, y1 = Y
+            return [(x0, y0), (x1, y1), (x0 + x1, y0 + y1)]
+        if self.kind == SQR:
+            return [(x0 + x1, x0 - x1 + K3P), (x0, x1)]
+        if self.kind == FPMUL:
+            y = Y[1] if self.yim else Y[0]
+            return [(x0, y), (x1, y)]
+        return [(x0, x0), (x1, x1)]
+
+
+class Out:
+    def __init__(self, dst, mode=M_SIMPLE, terms=(), lins=(), c_re=1, c_im=1):
+        self.dst, self.mode, self.terms, self.lins = dst, mode, list(terms), list(lins)
+        self.c_re, self.c_im = c_re, c_im
+        if mode == M_SIMPLE and (lins or c_re != 1 or c_im != 1):
+            self.mode = M_FULL
+        self.bias_re = self.bias_im = self.bias_lin_re = self.bias_lin_im = 0
+
+
+# ---------------------------------------------------------------- static bounds
+def _prod_bounds(t):
+    B = SLOT_BOUND
+    if t.kind == KARA:
+        return [B * B, B * B, 4 * B * B]
+    if t.kind == SQR:
+        return [2 * B * (B + K3P), B * B]
+    return [B * B, B * B]
+
+
+def finish(o):
+    """Fix the biases of an output from worst-case bounds and check limits."""
+    if o.mode in (M_SIMPLE, M_FULL):
+        pos = [0, 0]
+        neg = [0, 0]
+        for t in o.terms:
+            al, be = t.coefs()
+            for k, pb in enumerate(_prod_bounds(t)):
+                for c, co in enumerate((al[k], be[k])):
+                    if co > 0:
+                        pos[c] += co * pb
+                    else:
+                        neg[c] += -co * pb
+        o.bias_re = -(-neg[0] // (P * R))
+        o.bias_im = -(-neg[1] // (P * R))
+        for c, bk in enumerate((o.bias_re, o.bias_im)):
+            assert bk < 256
+            top = bk * P * R + pos[c]
+            assert top < ACC_LIMIT, "accumulator bound"
+            assert top // R + P < POST_LIMIT
+    if o.mode in (M_FULL, M_LIN):
+        for c, cc in enumerate((o.c_re, o.c_im)):
+            negs = poss = 0
+            if o.mode == M_FULL:      # c scales the REDC result, lins enter as they are
+                negs, poss = (-cc if cc < 0 else 0) * SLOT_BOUND, (cc if cc > 0 else 0) * SLOT_BOUND
+                mult = 1
+            else:                     # c scales every lin term
+                mult = cc
+            for co, _ in o.lins:
+                e = co * mult
+                if e < 0:
+                    negs += -e * SLOT_BOUND
+                else:
+                    poss += e * SLOT_BOUND
+            bk = -(-negs // P)
+            assert bk < 256
+            if c == 0:
+                o.bias_lin_re = bk
+            else:
+                o.bias_lin_im = bk
+            assert bk * P + poss < POST_LIMIT
+    return o
+
+
+# ---------------------------------------------------------------- tower helpers
+# tower position t (0..5: c0.c0, c0.c1, c0.c2, c1.c0, c1.c1, c1.c2) <-> power of w
+W_OF_T = [0, 2, 4, 1, 3, 5]
+T_OF_W = [W_OF_T.index(k) for k in range(6)]
+
+
+def prog_mul():
+    """D = A * B (field_sppark.cuh:142-146): w-basis schoolbook, lazily."""
+    outs = []
+    for t in range(6):
+        k = W_OF_T[t]
+        terms = []
+        for i in range(6):
+            j = (k - i) % 6
+            terms.append(Term(KARA, ref(B_A, T_OF_W[i]), ref(B_B, T_OF_W[j]), xi=int(i + j >= 6)))
+        outs.append(finish(Out(ref(B_D, t), terms=terms)))
+    return outs
+
+
+def prog_sqr():
+    """D = A^2 (field_sppark.cuh:148-151)."""
+    outs = []
+    for t in range(6):
+        k = W_OF_T[t]
+        terms = []
+        for i in range(6):
+            j = (k - i) % 6
+            if i > j:
+                continue
+            xi = int(i + j >= 6)
+            if i == j:
+                terms.append(Term(SQR, ref(B_A, T_OF_W[i]), xi=xi))
+            else:
+                terms.append(Term(KARA, ref(B_A, T_OF_W[i]), ref(B_A, T_OF_W[j]), xi=xi, dbl=1))
+        outs.append(finish(Out(ref(B_D, t), terms=terms)))
+    return outs
+
+
+def prog_line(pair):
+    """D = A * (l0 + l2 w^2 + l3 w^3), the sparse line product of
+    fp12_mul_by_014 (field_sppark.cuh:126-140) with l0 = c2, l2 = c1 * P.x,
+    l3 = c0 * P.y (api.cu:37-38)."""
+    o = 6 * pair
+    lref = {0: ref(B_C, o + C_C2), 2: ref(B_C, o + C_L2), 3: ref(B_C, o + C_L3)}
+    outs = []
+    for t in range(6):
+        k = W_OF_T[t]
+        terms = []
+        for j, lr in sorted(lref.items()):
+            i = (k - j) % 6
+            terms.append(Term(KARA, ref(B_A, T_OF_W[i]), lr, xi=int(k - j < 0)))
+        outs.append(finish(Out(ref(B_D, t), terms=terms)))
+    return outs
+
+
+def prog_lscale():
+    """l2 = c1 * P.x, l3 = c0 * P.y for both pairs (api.cu:37-38)."""
+    outs = []
+    for pair in range(2):
+        o = 6 * pair
+        outs.append(finish(Out(ref(B_C, o + C_L2), terms=[Term(FPMUL, ref(B_C, o + C_C1), ref(B_C, o + C_PT))])))
+        outs.append(finish(Out(ref(B_C, o + C_L3),
+                               terms=[Term(FPMUL, ref(B_C, o + C_C0), ref(B_C, o + C_PT), yim=1)])))
+    return outs + [None, None]
+
+
+def prog_cycsqr():
+    """D = Granger-Scott cyclotomic square of A (field_sppark.cuh:174-197)."""
+    z = {0: 0, 4: 1, 3: 2, 2: 3, 1: 4, 5: 5}   # z_i -> tower position
+    zr = {i: ref(B_A, t) for i, t in z.items()}
+    outs = [None] * 6
+
+    def sqr_out(i, a, b):     # z_i' = 3 (xi b^2 + a^2) - 2 z_i
+        return finish(Out(ref(B_D, z[i]), terms=[Term(SQR, zr[b], xi=1), Term(SQR, zr[a])],
+                          lins=[(-2, zr[i])], c_re=3, c_im=3))
+
+    def mul_out(i, a, b, xi):  # z_i' = 6 xi^e a b + 2 z_i
+        return finish(Out(ref(B_D, z[i]), terms=[Term(KARA, zr[a], zr[b], xi=xi)],
+                          lins=[(2, zr[i])], c_re=6, c_im=6))
+    outs[z[0]] = sqr_out(0, 0, 1)
+    outs[z[1]] = mul_out(1, 0, 1, 0)
+    outs[z[4]] = sqr_out(4, 2, 3)
+    outs[z[5]] = mul_out(5, 2, 3, 0)
+    outs[z[2]] = mul_out(2, 4, 5, 1)
+    outs[z[3]] = sqr_out(3, 4, 5)
+    return outs
+
+
+def prog_frob():
+    """D = Frobenius(A) (field_sppark.cuh:159-166): each coefficient is
+    conj(a_t) * g_t = conj(a_t * conj(g_t)), g in {1, k1, k2, k12, k1 k12, k2 k12}."""
+    gk = [None, K_FROB + 0, K_FROB + 1, K_FROB + 2, K_FROB + 3, K_FROB + 4]
+    outs = []
+    for t in range(6):
+        if gk[t] is None:
+            outs.append(finish(Out(ref(B_D, t), mode=M_LIN, lins=[(1, ref(B_A, t))], c_re=1, c_im=-1)))
+        else:
+            outs.append(finish(Out(ref(B_D, t), terms=[Term(KARA, ref(B_A, t), ref(B_K, gk[t]))], c_re=1, c_im=-1)))
+    return outs
+
+
+def prog_conj():
+    """D = conjugate(A) = c0 - c1 w."""
+    return [finish(Out(ref(B_D, t), mode=M_LIN, lins=[(1 if t < 3 else -1, ref(B_A, t))])) for t in range(6)]
+
+
+def prog_copy():
+    return [finish(Out(ref(B_D, t), mode=M_LIN, lins=[(1, ref(B_A, t))])) for t in range(6)]
+
+
+# Fp12 inverse (field_sppark.cuh:153-157 -> 104-111 -> 79-83 -> 40-50), in steps.
+# Temporaries (base T): 0-2 t = c0^2 - v c1^2, 3-5 (A, B, C), 6 F, 7 n, 8 n^-1,
+# 9 F^-1, 10-12 t^-1.
+def prog_inv1():
+    a = [ref(B_A, t) for t in range(3)]
+    b = [ref(B_A, 3 + t) for t in range(3)]
+    T = lambda *args, **kw: Term(*args, **kw)
+    o0 = Out(ref(B_T, 0), terms=[T(SQR, a[0]), T(KARA, a[1], a[2], xi=1, dbl=1), T(SQR, b[1], xi=1, sign=-1),
+                                 T(KARA, b[0], b[2], xi=1, dbl=1, sign=-1)])
+    o1 = Out(ref(B_T, 1), terms=[T(KARA, a[0], a[1], dbl=1), T(SQR, a[2], xi=1), T(SQR, b[0], sign=-1),
+                                 T(KARA, b[1], b[2], xi=1, dbl=1, sign=-1)])
+    o2 = Out(ref(B_T, 2), terms=[T(SQR, a[1]), T(KARA, a[0], a[2], dbl=1), T(KARA, b[0], b[1], dbl=1, sign=-1),
+                                 T(SQR, b[2], xi=1, sign=-1)])
+    return [finish(o0), finish(o1), finish(o2), None, None, None]
+
+
+def prog_inv2():
+    t = [ref(B_T, i) for i in range(3)]
+    oA = Out(ref(B_T, 3), terms=[Term(SQR, t[0]), Term(KARA, t[1], t[2], xi=1, sign=-1)])
+    oB = Out(ref(B_T, 4), terms=[Term(SQR, t[2], xi=1), Term(KARA, t[0], t[1], sign=-1)])
+    oC = Out(ref(B_T, 5), terms=[Term(SQR, t[1]), Term(KARA, t[0], t[2], sign=-1)])
+    return [finish(oA), finish(oB), finish(oC), None, None, None]
+
+
+def prog_inv3():
+    t = [ref(B_T, i) for i in range(3)]
+    A, B, C = ref(B_T, 3), ref(B_T, 4), ref(B_T, 5)
+    oF = Out(ref(B_T, 6), terms=[Term(KARA, t[0], A), Term(KARA, t[2], B, xi=1), Term(KARA, t[1], C, xi=1)])
+    return [finish(oF), None, None, None, None, None]
+
+
+def prog_inv4():
+    return [finish(Out(ref(B_T, 7), terms=[Term(NORM, ref(B_T, 6))])), None, None, None, None, None]
+
+
+def prog_inv5():
+    o = Out(ref(B_T, 8), mode=M_INVFP, lins=[(1, ref(B_T, 7))])
+    return [o, None, None, None, None, None]
+
+
+def prog_inv6():
+    o = Out(ref(B_T, 9), terms=[Term(FPMUL, ref(B_T, 6), ref(B_T, 8))], c_re=1, c_im=-1)
+    return [finish(o), None, None, None, None, None]
+
+
+def prog_inv7():
+    return [finish(Out(ref(B_T, 10 + i), terms=[Term(KARA, ref(B_T, 3 + i), ref(B_T, 9))])) for i in range(3)] + \
+        [None, None, None]
+
+
+def prog_inv8():
+    ti = [ref(B_T, 10 + i) for i in range(3)]
+    outs = []
+    for half in range(2):
+        x = [ref(B_A, 3 * half + i) for i in range(3)]
+        s = 1 if half == 0 else -1
+        # Fp6 product (x0 + x1 v + x2 v^2)(t0 + t1 v + t2 v^2), v^3 = xi
+        outs.append(finish(Out(ref(B_D, 3 * half + 0), terms=[Term(KARA, x[0], ti[0], sign=s),
+                                                            Term(KARA, x[1], ti[2], xi=1, sign=s),
+                                                            Term(KARA, x[2], ti[1], xi=1, sign=s)])))
+        outs.append(finish(Out(ref(B_D, 3 * half + 1), terms=[Term(KARA, x[0], ti[1], sign=s),
+                                                            Term(KARA, x[1], ti[0], sign=s),
+                                                            Term(KARA, x[2], ti[2], xi=1, sign=s)])))
+        outs.append(finish(Out(ref(B_D, 3 * half + 2), terms=[Term(KARA, x[0], ti[2], sign=s),
+                                                            Term(KARA, x[1], ti[1], sign=s),
+                                                            Term(KARA, x[2], ti[0], sign=s)])))
+    return outs
+
+
+PROGRAMS = [
+    ("LSCALE", prog_lscale, "C: l2 = c1 * P.x, l3 = c0 * P.y for both pairs (api.cu:37-38)"),
+    ("LINE1", lambda: prog_line(0), "D = A * line of pair 1 (field_sppark.cuh:126-140)"),
+    ("LINE2", lambda: prog_line(1), "D = A * line of pair 2"),
+    ("SQR", prog_sqr, "D = A^2 (field_sppark.cuh:148-151)"),
+    ("CYCSQR", prog_cycsqr, "D = cyclotomic square of A (field_sppark.cuh:174-197)"),
+    ("MUL", prog_mul, "D = A * B (field_sppark.cuh:142-146)"),
+    ("FROB", prog_frob, "D = Frobenius(A) (field_sppark.cuh:159-166)"),
+    ("CONJ", prog_conj, "D = conjugate(A)"),
+    ("COPY", prog_copy, "D = A"),
+    ("INV1", prog_inv1, "T0-2 = c0^2 - v c1^2 (field_sppark.cuh:153-157)"),
+    ("INV2", prog_inv2, "T3-5 = Fp6 inverse cofactors (field_sppark.cuh:104-111)"),
+    ("INV3", prog_inv3, "T6 = Fp6 norm to Fp2"),
+    ("INV4", prog_inv4, "T7 = Fp2 norm to Fp (field_sppark.cuh:79-83)"),
+    ("INV5", prog_inv5, "T8 = T7^-1 in Fp"),
+    ("INV6", prog_inv6, "T9 = T6^-1"),
+    ("INV7", prog_inv7, "T10-12 = Fp6 inverse"),
+    ("INV8", prog_inv8, "D = A^-1"),
+]
+
+
+def build():
+    progs = []
+    for name, fn, doc in PROGRAMS:
+        outs = fn()
+        assert len(outs) == 6
+        progs.append((name, outs, doc))
+    return progs
+
+
+# ---------------------------------------------------------------- emulator
+def redc(acc):
+    assert 0 <= acc < ACC_LIMIT
+    m = (-acc * pow(P, -1, R)) % R
+    r = (acc + m * P) >> 384
+    assert (acc + m * P) % R == 0
+    return r
+
+
+def qp(v):
+    assert 0 <= v < POST_LIMIT, hex(v)
+    r = v - QP[v >> 381]
+    assert 0 <= r < SLOT_BOUND
+    return r
+
+
+def fp_inv_mont(x):
+    """(x R^-1)^-1 R mod p, canonical; 0 for 0."""
+    x %= P
+    if x == 0:
+        return 0
+    return pow(x, -1, P) * R * R % P
+
+
+class Emulator:
+    """Slots: dict (absolute slot id) -> (re, im) integers.  `bases` maps the
+    base codes to absolute slot ids of index 0."""
+
+    def __init__(self, progs):
+        self.progs = {name: outs for name, outs, _ in progs}
+
+    @staticmethod
+    def _acc(terms, slots, bases, bias_k):
+        acc = [bias_k[0] * P * R, bias_k[1] * P * R]
+        for t in terms:
+            X = slots[bases[t.x >> 4] + (t.x & 15)]
+            Y = slots[bases[t.y >> 4] + (t.y & 15)] if t.y is not None else None
+            al, be = t.coefs()
+            for k, (u, v) in enumerate(t.operands(X, Y)):
+                assert 0 <= u < R and 0 <= v < R
+                pr = u * v
+                acc[0] += al[k] * pr
+                acc[1] += be[k] * pr
+        return acc
+
+    def run(self, name, slots, bases):
+        outs = self.progs[name]
+        res = []
+        for o in outs:
+            if o is None:
+                continue
+            if o.mode == M_INVFP:
+                z = slots[bases[o.lins[0][1] >> 4] + (o.lins[0][1] & 15)]
+                v = (fp_inv_mont(z[0]), 0)
+            elif o.mode == M_LIN:
+                v = []
+                for c, cc in enumerate((o.c_re, o.c_im)):
+                    s = (o.bias_lin_re, o.bias_lin_im)[c] * P
+                    for co, r in o.lins:
+                        s += cc * co * slots[bases[r >> 4] + (r & 15)][c]
+                    v.append(qp(s))
+                v = tuple(v)
+            else:
+                acc = self._acc(o.terms, slots, bases, (o.bias_re, o.bias_im))
+                r = [redc(a) for a in acc]
+                if o.mode == M_SIMPLE:
+                    v = (qp(r[0]), qp(r[1]))
+                else:
+                    v = []
+                    for c, cc in enumerate((o.c_re, o.c_im)):
+                        s = (o.bias_lin_re, o.bias_lin_im)[c] * P + cc * qp(r[c])
+                        for co, rr in o.lins:
+                            s += co * slots[bases[rr >> 4] + (rr & 15)][c]
+                        v.append(qp(s))
+                    v = tuple(v)
+            res.append((bases[o.dst >> 4] + (o.dst & 15), v))
+        for d, v in res:      # every lane computes before any writes
+            slots[d] = v
+
+
+# ---------------------------------------------------------------- constants
+def _f2_mul(a, b):
+    return ((a[0] * b[0] - a[1] * b[1]) % P, (a[0] * b[1] + a[1] * b[0]) % P)
+
+
+def _f2_pow(a, e):
+    r = (1, 0)
+    while e:
+        if e & 1:
+            r = _f2_mul(r, a)
+        a = _f2_mul(a, a)
+        e >>= 1
+    return r
+
+
+def frobenius_gammas():
+    """g1 = xi^((p-1)/3), g2 = xi^(2(p-1)/3), g12 = xi^((p-1)/6) (normal form):
+    the Frobenius constants of field_sppark.cuh:113-123 and 159-166."""
+    xi = (1, 1)
+    return _f2_pow(xi, (P - 1) // 3), _f2_pow(xi, 2 * (P - 1) // 3), _f2_pow(xi, (P - 1) // 6)
+
+
+def k_slot_values():
+    """Block-shared constant slots (Montgomery Fp2): 0, 1, then conj(g) for
+    g in k1, k2, k12, k1 k12, k2 k12, then 0."""
+    k1, k2, k12 = frobenius_gammas()
+    gs = [k1, k2, k12, _f2_mul(k1, k12), _f2_mul(k2, k12)]
+    mont = lambda v: v * R % P
+    out = [(0, 0), (mont(1), 0)] + [(mont(g[0]), mont(-g[1] % P)) for g in gs] + [(0, 0)]
+    return out
+
+
+def _limbs32(v, n=12):
+    return ["0x%08xu" % ((v >> (32 * i)) & 0xffffffff) for i in range(n)]
+
+
+# ---------------------------------------------------------------- C emission
+def encode_term(t):
+    w = t.kind | (t.xi << 2) | ((1 if t.sign < 0 else 0) << 3) | (t.dbl << 4) | (t.yim << 5)
+    w |= t.x << 8
+    w |= (t.y if t.y is not None else 0) << 16
+    return w
+
+
+def encode_out(o):
+    """header: mode | nterms << 2 | nlin << 6 | dst << 8 | (c_re & 15) << 16 | (c_im & 15) << 20
+       biases: re | im << 8 | lin_re << 16 | lin_im << 24; then terms, then lins (coef & 15 | ref << 8)."""
+    nt, nl = len(o.terms), len(o.lins)
+    assert nt < 16 and nl < 4
+    hdr = o.mode | (nt << 2) | (nl << 6) | (o.dst << 8) | ((o.c_re & 15) << 16) | ((o.c_im & 15) << 20)
+    bias = o.bias_re | (o.bias_im << 8) | (o.bias_lin_re << 16) | (o.bias_lin_im << 24)
+    words = [hdr, bias] + [encode_term(t) for t in o.terms] + [(co & 15) | (r << 8) for co, r in o.lins]
+    return words
+
+
+def emit(path):
+    progs = build()
+    L = ["// Generated by gen_fp2ops.py (Fp2-lane tower programs of the verify",
+         "// kernel); do not edit, run `python gen_fp2ops.py`.",
+         "#pragma once", "#include <cstdint>", "", "namespace bls {", "namespace f2 {", ""]
+    for i, (n, _, doc) in enumerate(progs):
+        L.append("constexpr int P_%s = %d;  // %s" % (n, i, doc))
+    L.append("constexpr int kNumPrograms = %d;" % len(progs))
+    L.append("constexpr uint32_t kModeSimple = %d, kModeFull = %d, kModeLin = %d, kModeInvFp = %d;"
+             % (M_SIMPLE, M_FULL, M_LIN, M_INVFP))
+    L.append("constexpr uint32_t kKara = %d, kSqr = %d, kFpMul = %d, kNorm = %d;" % (KARA, SQR, FPMUL, NORM))
+    L += ["constexpr int kKFrob = %d;" % K_FROB, ""]
+    words, index = [], []
+    for n, outs, _ in progs:
+        row = []
+        for o in outs:
+            if o is None:
+                row.append(0xffff)
+            else:
+                row.append(len(words))
+                words.extend(encode_out(o))
+        index.append(row)
+    L.append("// per program and lane: first word of the lane's output descriptor (0xffff: none)")
+    L.append("__device__ __constant__ uint16_t kOutIndex[%d][8] = {" % len(progs))
+    for (n, _, _), row in zip(progs, index):
+        L.append("    {%s, 0xffff, 0xffff},  // %s" % (", ".join("%d" % v for v in row), n))
+    L.append("};")
+    L.append("__device__ __constant__ uint32_t kDesc[%d] = {" % len(words))
+    for i in range(0, len(words), 6):
+        L.append("    " + ", ".join("0x%08xu" % w for w in words[i:i + 6]) + ",")
+    L.append("};")
+    L.append("// accumulator coefficients per (kind, xi): alpha0..2, beta0..2 as 4-bit two's complement")
+    L.append("__device__ __constant__ uint32_t kCoef[8] = {")
+    row = []
+    for kind in range(4):
+        for xi in range(2):
+            al, be = COEF.get((kind, xi), ((0, 0, 0), (0, 0, 0)))
+            al, be = list(al) + [0] * (3 - len(al)), list(be) + [0] * (3 - len(be))
+            w = 0
+            for k, v in enumerate(al + be):
+                w |= (v & 15) << (4 * k)
+            row.append("0x%08xu" % w)
+    L.append("    " + ", ".join(row) + ",")
+    L.append("};")
+    L.append("// block-shared constant slots (Montgomery Fp2, re then im): 0, 1, conj of the")
+    L.append("// Frobenius constants k1, k2, k12, k1 k12, k2 k12, 0")
+    ks = k_slot_values()
+    L.append("__device__ __constant__ uint32_t kKSlots[%d][24] = {" % len(ks))
+    for re, im in ks:
+        L.append("    {" + ", ".join(_limbs32(re) + _limbs32(im)) + "},")
+    L.append("};")
+    L.append("constexpr int kKSlotCount = %d;" % len(ks))
+    L.append("// R^3 mod p: u * R^3 * R^-1 = u R^2 turns a plain inverse into Montgomery form")
+    L.append("__device__ __constant__ uint32_t kR3[12] = {" + ", ".join(_limbs32(R * R * R % P)) + "};")
+    L.append("// 3p, the offset of SQR's x0 - x1 + 3p")
+    L.append("__device__ __constant__ uint32_t k3P[12] = {" + ", ".join(_limbs32(K3P)) + "};")
+    L.append("// QP[h] = floor(h * 2^381 / p) * p, 13 words padded to 16")
+    L.append("__device__ const uint32_t kQP2[128][16] = {")
+    for q in QP:
+        L.append("    {" + ", ".join("0x%08xu" % ((q >> (32 * i)) & 0xffffffff) for i in range(16)) + "},")
+    L.append("};")
+    L += ["", "}  // namespace f2", "}  // namespace bls"]
+    with open(path, "w") as f:
+        f.write("\n".join(L) + "\n")
+
+
+def summary():
+    out = []
+    for n, outs, _ in build():
+        prods = []
+        for o in outs:
+            if o is None or o.mode in (M_LIN, M_INVFP):
+                prods.append(0)
+            else:
+                prods.append(sum(NPROD[t.kind] for t in o.terms))
+        redcs = sum(2 for o in outs if o is not None and o.mode in (M_SIMPLE, M_FULL))
+        out.append("%-7s products per lane %s  (max %2d, total %3d), REDC %2d" % (n, prods, max(prods), sum(prods),
+                                                                                  redcs))
+    return out
+
+
+if __name__ == "__main__":
+    if "--summary" in sys.argv:
+        print("\n".join(summary()))
+    else:
+        emit(os.path.join(os.path.dirname(os.path.abspath(__file__)), "fp2ops.inc"))

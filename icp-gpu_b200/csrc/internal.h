@@ -27,9 +27,15 @@ struct VerifyArgs {
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
 cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStream_t s);
-// lane-parallel verify (verify_vm.cu); in_status: per-item decode status or NULL
+// lane-parallel verify; in_status: per-item decode status or NULL.  lanes 6
+// runs the Fp2-lane kernel (verify_fp2.cu), 2, 4 and 8 the interpreter of
+// per-Fp programs (verify_vm.cu).
 cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int blocks_per_sm,
                                 int sms, cudaStream_t s);
+cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, int blocks_per_sm, int sms,
+                              cudaStream_t s);
+size_t verify_fp2_smem_bytes();
+int verify_fp2_blocks_per_sm();
 size_t verify_lanes_smem_bytes(int lanes);
 // blocks of the lane-parallel kernel resident per SM (occupancy calculator)
 int verify_lanes_blocks_per_sm(int lanes);

@@ -73,7 +73,8 @@ extern "C" int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64
     if (n < 0 || n > bls::kMaxItems) return BLS_ERR_INVALID;
     if (n == 0) return BLS_OK;
     if (!sigs48 || !neg_hms || !g2_coeffs || !pk_tables || !pk_index || !results) return BLS_ERR_INVALID;
-    if (lanes_per_pairing != 2 && lanes_per_pairing != 4 && lanes_per_pairing != 8) return BLS_ERR_INVALID;
+    if (lanes_per_pairing != 2 && lanes_per_pairing != 4 && lanes_per_pairing != 6 && lanes_per_pairing != 8)
+        return BLS_ERR_INVALID;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* base = nullptr;
     if (bls::scratch_address(&base) != cudaSuccess) return BLS_ERR_CUDA;

@@ -114,7 +114,7 @@ struct bls_server {
             a.sig_xy = (const uint64_t*)s.d_xy;
             status = (const uint32_t*)s.d_st;
         }
-        int lanes = view.lanes > 1 ? view.lanes : 8;
+        int lanes = view.lanes > 1 ? view.lanes : 6;
         if (bls::launch_verify_lanes(a, status, lanes, view.blocks_per_sm, view.sms, st) ||
             cudaMemcpyAsync(s.h_res, s.d_res, n * 4, cudaMemcpyDeviceToHost, st) || cudaEventRecord(s.done, st))
             return BLS_ERR_CUDA;
@@ -223,7 +223,7 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
         }
     }
     // set up the kernel (shared-memory size, occupancy) before serving
-    bls::verify_lanes_blocks_per_sm(s->view.lanes > 1 ? s->view.lanes : 8);
+    bls::verify_lanes_blocks_per_sm(s->view.lanes > 1 ? s->view.lanes : 6);
     s->worker = std::thread([s] { s->run(); });
     *out = s;
     return BLS_OK;

@@ -1,0 +1,470 @@
+// Fp2-lane verify kernel: six lanes per verification, lane k producing the
+// k-th Fp2 coefficient of every Fp12 result from the generated descriptors
+// (fp2ops.inc, gen_fp2ops.py), with lazy reduction: all the Fp2 products that
+// feed one coefficient are summed exactly in two 832-bit accumulators and
+// reduced once.  Five verifications per warp (lanes 30 and 31 idle).
+//
+// Per verification (gpu-crypto/cuda/api.cu:80-91, api.cu:30-52, api.cu:65-78):
+//   Miller loop   for each of the 68 line coefficients: both pairs'
+//                 coefficients go to the C area, LSCALE forms c1 P.x and c0 P.y,
+//                 LINE1 and LINE2 multiply f by the two lines; 62 SQR in
+//                 between; CONJ at the end (x < 0)
+//   final exp     the reference's chain over 7 Fp12 groups, the inverse in 8
+//                 steps with an extended-Euclid Fp inverse on one lane
+//   result        canonical Gt compared with 1; optional Miller / Gt outputs
+//
+// Shared memory: 8 block-shared constant slots (0, 1, Frobenius constants),
+// then per pairing 7 groups of 6 Fp2 slots and a 12-slot C area (lines,
+// points).  An Fp2 slot is 24 words: re then im, each below 2^381 + p.  Every
+// program computes all outputs into registers, meets at __syncwarp, writes,
+// and meets again, so a program may overwrite its own inputs.
+#include <cuda_runtime.h>
+
+#include "fp2ops.cuh"
+#include "g1.cuh"
+#include "internal.h"
+
+namespace bls {
+namespace {
+
+constexpr uint64_t kXAbs = 0xd201000000010000ULL;
+constexpr int kLanes = 6;
+constexpr int kPairsPerWarp = 5;
+constexpr int kGroups = 7;
+constexpr int kTGroup = 3;                      // inversion temporaries: groups 3-5
+constexpr int kCOff = 6 * kGroups;              // C area after the groups
+constexpr int kPairSlots = kCOff + 12;          // Fp2 slots per pairing
+constexpr int kKSlots = f2::kKSlotCount;        // block-shared constants
+constexpr int kSlotWords = 24;
+
+struct Ctx {
+    uint32_t* sm;      // shared memory (words)
+    uint32_t region;   // first slot of this pairing
+    int lane;          // 0..5 within the pairing; 6, 7 for the idle lanes 30, 31
+    bool active;       // lane belongs to a pairing
+};
+
+struct Bases { uint32_t b[6]; };  // D, A, B, C, K, T: absolute slot of index 0
+
+__device__ __forceinline__ uint32_t grp(const Ctx& c, int g) { return c.region + 6 * g; }
+
+__device__ __forceinline__ uint32_t slot_addr(const Bases& bs, uint32_t ref) {
+    return bs.b[ref >> 4] + (ref & 15u);
+}
+
+__device__ __forceinline__ void load_fp(uint32_t* x, const uint32_t* sm, uint32_t slot, int comp) {
+    const uint4* s = reinterpret_cast<const uint4*>(sm + kSlotWords * slot + 12 * comp);
+    uint4 a = s[0], b = s[1], c = s[2];
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+    x[8] = c.x; x[9] = c.y; x[10] = c.z; x[11] = c.w;
+}
+__device__ __forceinline__ void store_fp(uint32_t* sm, uint32_t slot, int comp, const uint32_t* x) {
+    uint4* s = reinterpret_cast<uint4*>(sm + kSlotWords * slot + 12 * comp);
+    s[0] = make_uint4(x[0], x[1], x[2], x[3]);
+    s[1] = make_uint4(x[4], x[5], x[6], x[7]);
+    s[2] = make_uint4(x[8], x[9], x[10], x[11]);
+}
+
+__device__ __forceinline__ int sext4(uint32_t v) { return (int)(v << 28) >> 28; }
+
+// one output of a program: (re, im) into o0, o1
+__device__ __forceinline__ void compute_output(uint32_t off, const uint32_t* sm, const Bases& bs, uint32_t* o0,
+                                               uint32_t* o1) {
+    const uint32_t hdr = f2::kDesc[off], bias = f2::kDesc[off + 1];
+    const uint32_t mode = hdr & 3u, nt = (hdr >> 2) & 15u, nl = (hdr >> 6) & 3u;
+    const int c_re = sext4(hdr >> 16), c_im = sext4(hdr >> 20);
+    const uint32_t* lin = f2::kDesc + off + 2 + nt;
+
+    if (mode == f2::kModeInvFp) {
+        fp z;
+        load_fp(z.w, sm, slot_addr(bs, lin[0] >> 8), 0);
+        fp r = f2::fp_inverse_mont(z);
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+            o0[i] = r.w[i];
+            o1[i] = 0;
+        }
+        return;
+    }
+
+    uint32_t r[2][13];
+    if (mode == f2::kModeLin) {
+        for (int c = 0; c < 2; ++c) {
+            f2::set_kp(r[c], (bias >> (16 + 8 * c)) & 0xffu);
+            const int cc = c ? c_im : c_re;
+            for (uint32_t j = 0; j < nl; ++j) {
+                uint32_t z[12];
+                load_fp(z, sm, slot_addr(bs, lin[j] >> 8), c);
+                f2::madd13(r[c], z, cc * sext4(lin[j]));
+            }
+        }
+    } else {
+        uint32_t acc[2][26];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+            for (int i = 0; i < 12; ++i) acc[c][i] = 0;
+            acc[c][25] = 0;
+            f2::set_kp(acc[c] + 12, (bias >> (8 * c)) & 0xffu);
+        }
+        for (uint32_t t = 0; t < nt; ++t) {
+            const uint32_t w = f2::kDesc[off + 2 + t];
+            const uint32_t kind = w & 3u, xi = (w >> 2) & 1u, neg = (w >> 3) & 1u, dbl = (w >> 4) & 1u,
+                           yim = (w >> 5) & 1u;
+            const uint32_t xs = slot_addr(bs, (w >> 8) & 0x7fu), ys = slot_addr(bs, (w >> 16) & 0x7fu);
+            // operands of products 0 and 1: (A0, B0), (A1, B1); KARA's product 2 is (A0 + A1, B0 + B1)
+            uint32_t A0[12], A1[12], B0[12], B1[12];
+            load_fp(A0, sm, xs, 0);
+            load_fp(A1, sm, xs, 1);
+            if (kind == f2::kKara) {
+                load_fp(B0, sm, ys, 0);
+                load_fp(B1, sm, ys, 1);
+            } else if (kind == f2::kSqr) {
+                f2::add3p_sub(B0, A0, A1);      // x0 - x1 + 3p
+#pragma unroll
+                for (int i = 0; i < 12; ++i) B1[i] = A1[i];
+                uint32_t s[12];
+                f2::add12(s, A0, A1);
+#pragma unroll
+                for (int i = 0; i < 12; ++i) {
+                    A1[i] = A0[i];              // x0
+                    A0[i] = s[i];               // x0 + x1
+                }
+            } else if (kind == f2::kFpMul) {
+                load_fp(B0, sm, ys, yim);
+#pragma unroll
+                for (int i = 0; i < 12; ++i) B1[i] = B0[i];
+            } else {                            // NORM
+#pragma unroll
+                for (int i = 0; i < 12; ++i) {
+                    B0[i] = A0[i];
+                    B1[i] = A1[i];
+                }
+            }
+            const uint32_t cw = f2::kCoef[2 * kind + xi];
+            const int scale = (neg ? -1 : 1) * (dbl ? 2 : 1);
+            const uint32_t np = kind == f2::kKara ? 3u : 2u;
+#pragma unroll 1
+            for (uint32_t j = 0; j < np; ++j) {
+                uint32_t U[12], V[12];
+                if (j == 2) {
+                    f2::add12(U, A0, A1);
+                    f2::add12(V, B0, B1);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 12; ++i) {
+                        U[i] = j ? A1[i] : A0[i];
+                        V[i] = j ? B1[i] : B0[i];
+                    }
+                }
+                uint32_t P[24];
+                f2::prod24(P, U, V);
+                f2::acc_add(acc[0], P, scale * sext4(cw >> (4 * j)));
+                f2::acc_add(acc[1], P, scale * sext4(cw >> (4 * (3 + j))));
+            }
+        }
+        uint32_t red[2][13];
+        f2::redc26(red[0], acc[0]);
+        f2::redc26(red[1], acc[1]);
+        if (mode == f2::kModeSimple) {
+            f2::qp_reduce(o0, red[0]);
+            f2::qp_reduce(o1, red[1]);
+            return;
+        }
+        for (int c = 0; c < 2; ++c) {
+            uint32_t q[12];
+            f2::qp_reduce(q, red[c]);
+            f2::set_kp(r[c], (bias >> (16 + 8 * c)) & 0xffu);
+            f2::madd13(r[c], q, c ? c_im : c_re);
+            for (uint32_t j = 0; j < nl; ++j) {
+                uint32_t z[12];
+                load_fp(z, sm, slot_addr(bs, lin[j] >> 8), c);
+                f2::madd13(r[c], z, sext4(lin[j]));
+            }
+        }
+    }
+    f2::qp_reduce(o0, r[0]);
+    f2::qp_reduce(o1, r[1]);
+}
+
+// run program `pid` on the pairing: compute, meet, write, meet
+static __device__ __noinline__ void run(int pid, const Ctx& c, Bases bs) {
+    const uint32_t off = c.active ? f2::kOutIndex[pid][c.lane] : 0xffffu;
+    uint32_t o0[12], o1[12];
+    if (off != 0xffffu) compute_output(off, c.sm, bs, o0, o1);
+    __syncwarp();
+    if (off != 0xffffu) {
+        const uint32_t dst = slot_addr(bs, (f2::kDesc[off] >> 8) & 0x7fu);
+        store_fp(c.sm, dst, 0, o0);
+        store_fp(c.sm, dst, 1, o1);
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void call(const Ctx& c, int pid, int d, int a = 0, int b = 0) {
+    Bases bs;
+    bs.b[0] = grp(c, d);
+    bs.b[1] = grp(c, a);
+    bs.b[2] = grp(c, b);
+    bs.b[3] = c.region + kCOff;
+    bs.b[4] = 0;
+    bs.b[5] = grp(c, kTGroup);
+    run(pid, c, bs);
+}
+
+__device__ __forceinline__ void inverse(const Ctx& c, int d, int a) {
+    for (int k = f2::P_INV1; k <= f2::P_INV8; ++k) call(c, k, d, a);
+}
+
+__device__ __forceinline__ void copy_fp_from_global(uint32_t* sm, uint32_t slot, int comp, const uint64_t* src) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(sm + kSlotWords * slot + 12 * comp);
+    d[0] = __ldg(s);
+    d[1] = __ldg(s + 1);
+    d[2] = __ldg(s + 2);
+}
+
+// line coefficient `ci` of both pairs into the C area (lane k: pair k / 3,
+// coefficient k % 3), then LSCALE.  A skipped pair gets the line (0, 0, 1),
+// which leaves f unchanged.
+__device__ __forceinline__ void load_lines(const Ctx& c, const uint64_t* q1, bool skip1, const uint64_t* q2,
+                                           bool skip2, int ci) {
+    if (c.active) {
+        const int pair = c.lane / 3, k = c.lane % 3;
+        const uint64_t* q = pair ? q2 : q1;
+        const bool skip = pair ? skip2 : skip1;
+        const uint32_t slot = c.region + kCOff + 6 * pair + k;
+        if (skip) {
+            fp v = k == 2 ? fp_one() : fp_zero();
+            store_fp(c.sm, slot, 0, v.w);
+            store_fp(c.sm, slot, 1, fp_zero().w);
+        } else {
+            copy_fp_from_global(c.sm, slot, 0, q + 36 * ci + 12 * k);
+            copy_fp_from_global(c.sm, slot, 1, q + 36 * ci + 12 * k + 6);
+        }
+    }
+    __syncwarp();
+    call(c, f2::P_LSCALE, 0);
+}
+
+__device__ __forceinline__ void line_step(const Ctx& c, const uint64_t* q1, bool skip1, const uint64_t* q2,
+                                          bool skip2, int ci) {
+    load_lines(c, q1, skip1, q2, skip2, ci);
+    call(c, f2::P_LINE1, 0, 0);
+    call(c, f2::P_LINE2, 0, 0);
+}
+
+__device__ __forceinline__ void cyc_exp(const Ctx& c, int dst, int x, int spare) {
+    call(c, f2::P_COPY, dst, x);
+    int cur = dst, oth = spare;
+    for (int i = 62; i >= 0; --i) {
+        call(c, f2::P_CYCSQR, cur, cur);
+        if ((kXAbs >> i) & 1) {
+            call(c, f2::P_MUL, oth, cur, x);
+            int t = cur; cur = oth; oth = t;
+        }
+    }
+    call(c, f2::P_CONJ, dst, cur);
+}
+
+// final exponentiation of group 0 into group 0 (api.cu:65-78)
+__device__ __forceinline__ void final_exp(const Ctx& c) {
+    call(c, f2::P_CONJ, 1, 0);       // t0 = conj(f)            G1
+    inverse(c, 2, 0);                // t1 = f^-1               G2
+    call(c, f2::P_MUL, 3, 1, 2);     // t2 = t0 t1              G3
+    call(c, f2::P_FROB, 0, 3);
+    call(c, f2::P_FROB, 1, 0);       // frob^2(t2)              G1
+    call(c, f2::P_MUL, 2, 1, 3);     // t2 = frob^2(t2) t2      G2 (f = t2)
+    call(c, f2::P_COPY, 0, 2);
+    call(c, f2::P_CYCSQR, 0, 0);
+    call(c, f2::P_CONJ, 0, 0);       // t1 = conj(cyc_sqr(t2))  G0
+    cyc_exp(c, 1, 2, 3);             // t3 = cyc_exp(t2)        G1
+    call(c, f2::P_MUL, 3, 0, 1);     // t4 = t1 t3              G3
+    cyc_exp(c, 0, 3, 4);             // t1 = cyc_exp(t4)        G0
+    call(c, f2::P_CONJ, 3, 3);       // t4 = conj(t4)
+    call(c, f2::P_MUL, 4, 2, 3);     // f = f t4                G4
+    call(c, f2::P_COPY, 3, 1);
+    call(c, f2::P_CYCSQR, 3, 3);     // t4 = cyc_sqr(t3)        G3
+    cyc_exp(c, 5, 0, 6);             // t0 = cyc_exp(t1)        G5
+    call(c, f2::P_MUL, 6, 1, 5);     // t3 = t3 t0              G6
+    call(c, f2::P_FROB, 1, 6);
+    call(c, f2::P_FROB, 6, 1);       // t3 = frob^2(t3)         G6
+    call(c, f2::P_MUL, 1, 4, 6);     // f = f t3                G1
+    cyc_exp(c, 4, 5, 6);             // c = cyc_exp(t0)         G4
+    call(c, f2::P_MUL, 5, 3, 4);     // t4 = t4 c               G5
+    cyc_exp(c, 3, 5, 4);             // c = cyc_exp(t4)         G3
+    call(c, f2::P_MUL, 4, 1, 3);     // f = f c                 G4
+    call(c, f2::P_CONJ, 1, 2);       // conj(t2)                G1
+    call(c, f2::P_MUL, 3, 5, 1);     // t4 = t4 conj(t2)        G3
+    call(c, f2::P_MUL, 1, 2, 0);     // t2 = t2 t1              G1
+    call(c, f2::P_FROB, 0, 1);
+    call(c, f2::P_FROB, 2, 0);
+    call(c, f2::P_FROB, 0, 2);       // t2 = frob^3(t2)         G0
+    call(c, f2::P_MUL, 1, 4, 0);     // f = f t2                G1
+    call(c, f2::P_FROB, 2, 3);       // t4 = frob(t4)           G2
+    call(c, f2::P_MUL, 0, 1, 2);     // f = f t4                G0
+}
+
+// canonical form of a slot value (below 2^381 + p < 3p)
+__device__ __forceinline__ fp canonical(fp v) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        uint32_t d[12];
+        uint32_t br = sub_p(d, v.w);
+#pragma unroll
+        for (int i = 0; i < 12; ++i) v.w[i] = br ? v.w[i] : d[i];
+    }
+    return v;
+}
+
+// canonical group `g` -> out (72 u64) and the "is one" test over the pairing's lanes
+__device__ __forceinline__ bool emit_group(const Ctx& c, int g, uint64_t* out) {
+    bool ok = true;
+    if (c.active) {
+        fp re, im;
+        load_fp(re.w, c.sm, grp(c, g) + c.lane, 0);
+        load_fp(im.w, c.sm, grp(c, g) + c.lane, 1);
+        re = canonical(re);
+        im = canonical(im);
+        if (out) {
+            fp_store_u64(out + 12 * c.lane, re);
+            fp_store_u64(out + 12 * c.lane + 6, im);
+        }
+        ok = (c.lane == 0 ? fp_eq(re, fp_one()) : fp_is_zero(re)) && fp_is_zero(im);
+    }
+    const unsigned bad = __ballot_sync(0xffffffffu, !ok);
+    const unsigned lane32 = threadIdx.x & 31u;
+    const unsigned first = lane32 - (unsigned)c.lane;
+    const unsigned mask = c.active ? (0x3fu << first) : 0u;
+    return (bad & mask) == 0;
+}
+
+constexpr int kWarpsPerBlock = 1;
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_verify_fp2(VerifyArgs a, const uint32_t* __restrict__ in_status) {
+    extern __shared__ uint4 smem4[];
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem4);
+    const int warps = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane32 = threadIdx.x & 31;
+    const int pi = lane32 / kLanes;
+
+    for (int i = threadIdx.x; i < kKSlots * kSlotWords; i += blockDim.x) sm[i] = f2::kKSlots[i / kSlotWords][i % kSlotWords];
+    __syncthreads();
+
+    Ctx c;
+    c.sm = sm;
+    c.active = pi < kPairsPerWarp;
+    c.lane = c.active ? lane32 % kLanes : 6 + (lane32 & 1);
+    c.region = kKSlots + (warp * kPairsPerWarp + (c.active ? pi : 0)) * kPairSlots;
+
+    int next = (blockIdx.x * warps + warp) * kPairsPerWarp;
+    const int stride = gridDim.x * warps * kPairsPerWarp;
+    for (;;) {
+        int base;
+        if (a.work_counter) {
+            int b = 0;
+            if (lane32 == 0) b = atomicAdd(a.work_counter, kPairsPerWarp);
+            base = __shfl_sync(0xffffffffu, b, 0);
+        } else {
+            base = next;
+            next += stride;
+        }
+        if (base >= a.n) break;
+        const int item = base + (c.active ? pi : 0);
+        const bool have = c.active && item < a.n;
+        bool skip1 = true, skip2 = true;
+        const uint64_t* pk = a.g2;
+        int32_t status = 0;
+        if (have) {
+            const uint64_t* s = a.sig_xy ? a.sig_xy + 12 * (size_t)item : (const uint64_t*)a.sigs + 12 * (size_t)item;
+            const uint64_t* h = a.nhms + 12 * (size_t)item;
+            if (in_status) status = (int32_t)in_status[item];
+            fp sx = fp_load_u64(s), sy = fp_load_u64(s + 6);
+            fp hx = fp_load_u64(h), hy = fp_load_u64(h + 6);
+            int64_t pki = a.pk_index ? (int64_t)a.pk_index[item] : (int64_t)item;
+            pk = a.pk_tables + kCoeffU64 * pki;
+            skip1 = g1_limbs_identity(sx, sy) || status != 0;
+            skip2 = g1_limbs_identity(hx, hy) || (a.pk_identity && a.pk_identity[pki]) || status != 0;
+            if (c.lane == 0) {
+                const uint32_t C = c.region + kCOff;
+                store_fp(sm, C + 0 * 6 + 3, 0, skip1 ? fp_zero().w : sx.w);
+                store_fp(sm, C + 0 * 6 + 3, 1, skip1 ? fp_zero().w : sy.w);
+                store_fp(sm, C + 1 * 6 + 3, 0, skip2 ? fp_zero().w : hx.w);
+                store_fp(sm, C + 1 * 6 + 3, 1, skip2 ? fp_zero().w : hy.w);
+            }
+        } else if (c.active && c.lane == 0) {
+            const uint32_t C = c.region + kCOff;
+            for (int pair = 0; pair < 2; ++pair) {
+                store_fp(sm, C + pair * 6 + 3, 0, fp_zero().w);
+                store_fp(sm, C + pair * 6 + 3, 1, fp_zero().w);
+            }
+        }
+        // f = 1
+        if (c.active) {
+            store_fp(sm, grp(c, 0) + c.lane, 0, c.lane == 0 ? fp_one().w : fp_zero().w);
+            store_fp(sm, grp(c, 0) + c.lane, 1, fp_zero().w);
+        }
+        __syncwarp();
+
+        // Miller loop over |x| >> 1 below its leading bit (api.cu:30-52)
+        int ci = 0;
+        for (int b = 61; b >= 0; --b) {
+            line_step(c, a.g2, skip1, pk, skip2, ci++);
+            if (((kXAbs >> 1) >> b) & 1) line_step(c, a.g2, skip1, pk, skip2, ci++);
+            call(c, f2::P_SQR, 0, 0);
+        }
+        line_step(c, a.g2, skip1, pk, skip2, ci);
+        call(c, f2::P_CONJ, 0, 0);
+        if (a.ml_out) emit_group(c, 0, have ? a.ml_out + 72 * (size_t)item : nullptr);
+
+        final_exp(c);
+        const bool one = emit_group(c, 0, (have && a.gt_out) ? a.gt_out + 72 * (size_t)item : nullptr);
+        if (have && c.lane == 0) a.results[item] = status != 0 ? -status : (one ? 1 : 0);
+        __syncwarp();
+    }
+}
+
+size_t smem_bytes() {
+    return (size_t)(kKSlots + kWarpsPerBlock * kPairsPerWarp * kPairSlots) * kSlotWords * 4;
+}
+
+cudaError_t configure() {
+    static cudaError_t done =
+        cudaFuncSetAttribute(k_verify_fp2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes());
+    return done;
+}
+
+int resident() {
+    if (configure() != cudaSuccess) return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_verify_fp2, 32 * kWarpsPerBlock, smem_bytes()) !=
+        cudaSuccess)
+        return 0;
+    return blocks;
+}
+
+}  // namespace
+
+size_t verify_fp2_smem_bytes() { return smem_bytes(); }
+
+int verify_fp2_blocks_per_sm() { return resident(); }
+
+cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, int blocks_per_sm, int sms,
+                              cudaStream_t s) {
+    if (a.n <= 0) return cudaSuccess;
+    cudaError_t e = configure();
+    if (e != cudaSuccess) return e;
+    const int per_block = kWarpsPerBlock * kPairsPerWarp;
+    const int need = (a.n + per_block - 1) / per_block;
+    const int res = resident();
+    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm : (res > 0 ? res : 1);
+    const int cap = per_sm * sms;
+    int blocks = a.work_counter ? cap : (need < cap || blocks_per_sm <= 0 ? need : cap);
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    k_verify_fp2<<<blocks, 32 * kWarpsPerBlock, smem_bytes(), s>>>(a, in_status);
+    return cudaGetLastError();
+}
+
+}  // namespace bls

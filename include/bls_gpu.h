@@ -112,8 +112,10 @@ typedef struct {
     size_t mem_cap_bytes;   /* device-memory budget for this context (0 = none) */
     int threads_per_block;  /* 0 = library default */
     int blocks_per_sm;      /* persistent launches: 0 = occupancy maximum */
-    int lanes_per_pairing;  /* 1: one thread per verification; 2, 4, 8: that many lanes
-                               share one verification (0 = 8) */
+    int lanes_per_pairing;  /* 6 (default, 0): six lanes per verification, one per Fp2
+                               coefficient, lazy reduction (the fastest kernel);
+                               2, 4, 8: lanes share per-Fp operations of one
+                               verification; 1: one thread per verification */
 } bls_config;
 
 typedef struct {
@@ -231,7 +233,7 @@ int bls_server_stats(bls_server* srv, uint64_t* launches, uint64_t* items, uint6
  * (more returns BLS_ERR_INVALID).  All calls on a device share that array:
  * calls whose work overlaps on the GPU race and must be ordered by the
  * caller.  The first call on a device looks up the array's address; make it
- * before any stream capture.  lanes_per_pairing: 2, 4 or 8. */
+ * before any stream capture.  lanes_per_pairing: 2, 4, 6 or 8. */
 #define BLS_NOALLOC_MAX_ITEMS 8192
 int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64_t* neg_hms, const uint64_t* g2_coeffs,
                                   const uint64_t* pk_tables, const int32_t* pk_index, int32_t* results, int n,

@@ -1,0 +1,139 @@
+"""Python re-statement of the Fp2-lane verify kernel's driver (verify_fp2.cu)
+over the generated descriptor tables (gen_fp2ops.py), bit-exact with the
+device arithmetic: the same accumulators, biases, reductions and slot plan.
+Test infrastructure: lets the CPU suite check the tables, the bounds and the
+group plan of the final exponentiation against the oracle without a GPU."""
+import os
+import sys
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "icp-gpu_b200", "csrc"))
+import gen_fp2ops as G  # noqa: E402
+
+import bls_ref as B  # noqa: E402
+
+X_ABS = 0xD201000000010000
+K_SLOTS = 8
+GROUPS = 7
+T_GROUP = 3          # inversion temporaries start at group 3 (13 slots)
+C_OFF = 6 * GROUPS   # C area after the groups
+
+
+def mont(x):
+    return x * G.R % G.P
+
+
+def f2m(a):
+    return (mont(a[0]), mont(a[1]))
+
+
+def frob_constants():
+    """conj(g) for g in k1, k2, k12, k1 k12, k2 k12 (Montgomery Fp2)."""
+    k1, k2, k12 = B.FROB6_C1, B.FROB6_C2, B.FROB12_C1
+    gs = [k1, k2, k12, B.f2_mul(k1, k12), B.f2_mul(k2, k12)]
+    return [f2m(B.f2_conj(g)) for g in gs]
+
+
+class Machine:
+    def __init__(self):
+        self.e = G.Emulator(G.build())
+        self.slots = {}
+        ks = G.k_slot_values()
+        for i, v in enumerate(ks):
+            self.slots[i] = v
+        self.region = K_SLOTS
+        for s in range(self.region, self.region + C_OFF + 12):
+            self.slots[s] = (0, 0)
+
+    def grp(self, g):
+        return self.region + 6 * g
+
+    def call(self, name, d, a=0, b=0):
+        bases = [self.grp(d), self.grp(a), self.grp(b), self.region + C_OFF, 0, self.grp(T_GROUP)]
+        self.e.run(name, self.slots, bases)
+
+    def inv(self, d, a):
+        for k in range(1, 8):
+            self.call("INV%d" % k, d, a)
+        self.call("INV8", d, a)
+
+    def set_group(self, g, f2s):
+        for i, v in enumerate(f2s):
+            self.slots[self.grp(g) + i] = v
+
+    def group_flat(self, g):
+        out = []
+        for i in range(6):
+            re, im = self.slots[self.grp(g) + i]
+            out += [re % G.P, im % G.P]
+        return out
+
+
+def cyc_exp(m, dst, x, spare):
+    m.call("COPY", dst, x)
+    cur, oth = dst, spare
+    for i in range(62, -1, -1):
+        m.call("CYCSQR", cur, cur)
+        if (X_ABS >> i) & 1:
+            m.call("MUL", oth, cur, x)
+            cur, oth = oth, cur
+    m.call("CONJ", dst, cur)
+
+
+def final_exp(m):
+    c = m.call
+    c("CONJ", 1, 0); m.inv(2, 0); c("MUL", 3, 1, 2); c("FROB", 0, 3); c("FROB", 1, 0); c("MUL", 2, 1, 3)
+    c("COPY", 0, 2); c("CYCSQR", 0, 0); c("CONJ", 0, 0)
+    cyc_exp(m, 1, 2, 3)
+    c("MUL", 3, 0, 1)
+    cyc_exp(m, 0, 3, 4)
+    c("CONJ", 3, 3); c("MUL", 4, 2, 3); c("COPY", 3, 1); c("CYCSQR", 3, 3)
+    cyc_exp(m, 5, 0, 6)
+    c("MUL", 6, 1, 5); c("FROB", 1, 6); c("FROB", 6, 1); c("MUL", 1, 4, 6)
+    cyc_exp(m, 4, 5, 6)
+    c("MUL", 5, 3, 4)
+    cyc_exp(m, 3, 5, 4)
+    c("MUL", 4, 1, 3); c("CONJ", 1, 2); c("MUL", 3, 5, 1); c("MUL", 1, 2, 0)
+    c("FROB", 0, 1); c("FROB", 2, 0); c("FROB", 0, 2); c("MUL", 1, 4, 0); c("FROB", 2, 3); c("MUL", 0, 1, 2)
+
+
+def verify(sig, nhm, g2_limbs, pk_limbs, skip1=False, skip2=False):
+    """sig / nhm: canonical affine points; tables: 2448 u64.  Returns
+    (miller, gt) as canonical flat Fp lists (normal form)."""
+    m = Machine()
+    C = m.region + C_OFF
+    one = mont(1)
+    pts = [(0, 0) if skip1 else sig, (0, 0) if skip2 else nhm]
+    for pair in range(2):
+        m.slots[C + 6 * pair + G.C_PT] = (mont(pts[pair][0]), mont(pts[pair][1]))
+    m.set_group(0, [(one, 0)] + [(0, 0)] * 5)
+
+    def load(ci):
+        for pair, (tab, skip) in enumerate(((g2_limbs, skip1), (pk_limbs, skip2))):
+            for k in range(3):
+                if skip:
+                    v = (one, 0) if k == 2 else (0, 0)
+                else:
+                    w = [int(x) for x in tab[36 * ci + 12 * k: 36 * ci + 12 * k + 12]]
+                    v = (sum(x << (64 * i) for i, x in enumerate(w[:6])), sum(x << (64 * i) for i, x in enumerate(w[6:])))
+                m.slots[C + 6 * pair + k] = v
+        m.call("LSCALE", 0)
+
+    def lines():
+        m.call("LINE1", 0, 0)
+        m.call("LINE2", 0, 0)
+
+    ci = 0
+    for b in range(61, -1, -1):
+        load(ci); ci += 1
+        lines()
+        if ((X_ABS >> 1) >> b) & 1:
+            load(ci); ci += 1
+            lines()
+        m.call("SQR", 0, 0)
+    load(ci)
+    lines()
+    m.call("CONJ", 0, 0)
+    ml = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]
+    final_exp(m)
+    gt = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]
+    return ml, gt

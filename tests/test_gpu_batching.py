@@ -25,7 +25,7 @@ def _requests(ctx, wl):
     return reqs
 
 
-@pytest.mark.parametrize("lanes", [8, 4])
+@pytest.mark.parametrize("lanes", [6, 8, 4])
 def test_persistent_equals_plain_and_expected(wl, lanes):
     with G.Context(lanes=lanes) as ctx:
         reqs = _requests(ctx, wl)

@@ -11,7 +11,7 @@ import workload_py as W
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=[8, 4, 1], ids=["lanes8", "lanes4", "thread"])
+@pytest.fixture(scope="module", params=[6, 8, 4, 1], ids=["fp2lanes6", "lanes8", "lanes4", "thread"])
 def ctx(request):
     G.init()
     with G.Context(lanes=request.param) as c:
