@@ -22,21 +22,13 @@ __device__ __forceinline__ void prod24(uint32_t* p, const uint32_t* a, const uin
     }
 }
 
-// acc[0..25] += coef * p (coef in {-4, -2, -1, 0, 1, 2, 4}), modulo 2^832.
-// The operand is (p << s) masked to zero for coef == 0 and complemented for a
-// negative coef, with the complement's +1 entering as the first carry.
-__device__ __forceinline__ void acc_add(uint32_t* acc, const uint32_t* p, int coef) {
-    const int mag = coef < 0 ? -coef : coef;
-    const uint32_t s = mag >> 1;                    // 1 -> 0, 2 -> 1, 4 -> 2
-    const uint32_t z = coef != 0 ? 0xffffffffu : 0u;
-    const uint32_t m = coef < 0 ? 0xffffffffu : 0u;
-    uint32_t v[26];
-    v[0] = ((p[0] << s) & z) ^ m;
+// acc[0..25] += p (neg = 0) or -= p (neg = 1), modulo 2^832: the operand is
+// p complemented for a subtraction, with the complement's +1 as the first carry.
+__device__ __forceinline__ void acc_add(uint32_t* acc, const uint32_t* p, uint32_t neg) {
+    const uint32_t m = 0u - neg;
+    uint32_t v[24];
 #pragma unroll
-    for (int i = 1; i < 24; ++i) v[i] = (__funnelshift_l(p[i - 1], p[i], s) & z) ^ m;
-    v[24] = (__funnelshift_l(p[23], 0u, s) & z) ^ m;
-    v[25] = m;
-    const uint32_t cin = m & 1u;
+    for (int i = 0; i < 24; ++i) v[i] = p[i] ^ m;
     uint32_t dummy;
     asm("add.cc.u32 %26, %27, 0xffffffff;\n\t"
         "addc.cc.u32 %0, %0, %28;\n\t"
@@ -64,15 +56,22 @@ __device__ __forceinline__ void acc_add(uint32_t* acc, const uint32_t* p, int co
         "addc.cc.u32 %22, %22, %50;\n\t"
         "addc.cc.u32 %23, %23, %51;\n\t"
         "addc.cc.u32 %24, %24, %52;\n\t"
-        "addc.u32 %25, %25, %53;"
+        "addc.u32 %25, %25, %52;"
         : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3]), "+r"(acc[4]), "+r"(acc[5]), "+r"(acc[6]),
           "+r"(acc[7]), "+r"(acc[8]), "+r"(acc[9]), "+r"(acc[10]), "+r"(acc[11]), "+r"(acc[12]), "+r"(acc[13]),
           "+r"(acc[14]), "+r"(acc[15]), "+r"(acc[16]), "+r"(acc[17]), "+r"(acc[18]), "+r"(acc[19]),
           "+r"(acc[20]), "+r"(acc[21]), "+r"(acc[22]), "+r"(acc[23]), "+r"(acc[24]), "+r"(acc[25]), "=r"(dummy)
-        : "r"(cin), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+        : "r"(neg), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
           "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]),
           "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]),
-          "r"(v[24]), "r"(v[25]));
+          "r"(m));
+}
+
+// x = 2 x (12 limbs; x below 2^383)
+__device__ __forceinline__ void dbl12(uint32_t* x) {
+#pragma unroll
+    for (int i = 11; i > 0; --i) x[i] = __funnelshift_l(x[i - 1], x[i], 1);
+    x[0] <<= 1;
 }
 
 // t[0..12] = k * p for a small k (k < 2^32)

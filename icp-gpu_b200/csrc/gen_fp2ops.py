@@ -17,13 +17,14 @@ product; no intermediate result is rounded to Fp.
 
 Term kinds (X, Y are Fp2 slots, x0/x1 their components):
   KARA   X*Y          U = (x0, x1, x0+x1)  V = (y0, y1, y0+y1)
-  SQR    X^2          U = (x0+x1, x0)      V = (x0-x1+3p, x1)
+  SQR    X^2          U = (x0+x1, 2 x0)    V = (x0-x1+3p, x1)
   FPMUL  X*y (y in Fp) U = (x0, x1)        V = (y, y)
   NORM   x0^2+x1^2    U = (x0, x1)         V = (x0, x1)
-with per-product accumulator coefficients (alpha for ACC_re, beta for ACC_im)
-fixed by the kind and by `xi` (multiply the term by xi = 1 + u), then scaled by
-the term's sign and doubling.  Additive multiples of p (the 3p above, the
-biases) leave every value unchanged mod p.
+A KARA term times xi = 1 + u takes xi X = (x0 - x1 + 3p, x0 + x1) as its X; a
+doubled KARA term takes 2 Y as its Y.  The per-product accumulator
+coefficients (alpha for ACC_re, beta for ACC_im) are then all in {-1, 0, 1},
+fixed by the kind and `xi`, and negated for a negative term.  Additive
+multiples of p (the 3p above, the biases) leave every value unchanged mod p.
 
 Post-processing of an output:
   SIMPLE  out = QP(r)                               r = REDC result
@@ -73,9 +74,9 @@ KARA, SQR, FPMUL, NORM = range(4)
 # (alpha, beta) per product, plain and times xi
 COEF = {
     (KARA, 0): ((1, -1, 0), (-1, -1, 1)),
-    (KARA, 1): ((2, 0, -1), (0, -2, 1)),
-    (SQR, 0): ((1, 0), (0, 2)),
-    (SQR, 1): ((1, -2), (1, 2)),
+    (KARA, 1): ((1, -1, 0), (-1, -1, 1)),     # xi applied to X
+    (SQR, 0): ((1, 0), (0, 1)),                # second product is (2 x0) x1
+    (SQR, 1): ((1, -1), (1, 1)),
     (FPMUL, 0): ((1, 0), (0, 1)),
     (FPMUL, 1): ((1, -1), (1, 1)),
     (NORM, 0): ((1, 1), (0, 0)),
@@ -92,20 +93,24 @@ class Term:
         if kind in (SQR, NORM):
             self.y = x
         assert not (kind == NORM and xi)
+        assert not (dbl and kind != KARA)
 
     def coefs(self):
         a, b = COEF[(self.kind, self.xi)]
-        m = self.sign * (2 if self.dbl else 1)
-        return [m * v for v in a], [m * v for v in b]
+        return [self.sign * v for v in a], [self.sign * v for v in b]
 
     def operands(self, X, Y):
         """(U, V) integer pairs for the products, from component values."""
         x0, x1 = X
         if self.kind == KARA:
+            if self.xi:
+                x0, x1 = x0 - x1 + K3P, x0 + x1
             y0, y1 = Y
+            if self.dbl:
+                y0, y1 = 2 * y0, 2 * y1
             return [(x0, y0), (x1, y1), (x0 + x1, y0 + y1)]
         if self.kind == SQR:
-            return [(x0 + x1, x0 - x1 + K3P), (x0, x1)]
+            return [(x0 + x1, x0 - x1 + K3P), (2 * x0, x1)]
         if self.kind == FPMUL:
             y = Y[1] if self.yim else Y[0]
             return [(x0, y), (x1, y)]
@@ -122,13 +127,24 @@ class Out:
 
 
 # ---------------------------------------------------------------- static bounds
-def _prod_bounds(t):
+def _operand_bounds(t):
+    """exclusive upper bounds of (U, V) per product"""
     B = SLOT_BOUND
     if t.kind == KARA:
-        return [B * B, B * B, 4 * B * B]
+        bx0, bx1 = (B + K3P, 2 * B) if t.xi else (B, B)
+        by = 2 * B if t.dbl else B
+        return [(bx0, by), (bx1, by), (bx0 + bx1, 2 * by)]
     if t.kind == SQR:
-        return [2 * B * (B + K3P), B * B]
-    return [B * B, B * B]
+        return [(2 * B, B + K3P), (2 * B, B)]
+    return [(B, B), (B, B)]
+
+
+def _prod_bounds(t):
+    out = []
+    for bu, bv in _operand_bounds(t):
+        assert bu <= R and bv <= R, "operand bound"
+        out.append(bu * bv)
+    return out
 
 
 def finish(o):

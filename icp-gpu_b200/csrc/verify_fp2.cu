@@ -120,15 +120,27 @@ __device__ __forceinline__ void compute_output(uint32_t off, const uint32_t* sm,
             if (kind == f2::kKara) {
                 load_fp(B0, sm, ys, 0);
                 load_fp(B1, sm, ys, 1);
+                if (xi) {                       // X = xi X = (x0 - x1 + 3p, x0 + x1)
+                    uint32_t s[12];
+                    f2::add12(s, A0, A1);
+                    f2::add3p_sub(A0, A0, A1);
+#pragma unroll
+                    for (int i = 0; i < 12; ++i) A1[i] = s[i];
+                }
+                if (dbl) {
+                    f2::dbl12(B0);
+                    f2::dbl12(B1);
+                }
             } else if (kind == f2::kSqr) {
                 f2::add3p_sub(B0, A0, A1);      // x0 - x1 + 3p
 #pragma unroll
                 for (int i = 0; i < 12; ++i) B1[i] = A1[i];
                 uint32_t s[12];
                 f2::add12(s, A0, A1);
+                f2::dbl12(A0);
 #pragma unroll
                 for (int i = 0; i < 12; ++i) {
-                    A1[i] = A0[i];              // x0
+                    A1[i] = A0[i];              // 2 x0
                     A0[i] = s[i];               // x0 + x1
                 }
             } else if (kind == f2::kFpMul) {
@@ -142,8 +154,8 @@ __device__ __forceinline__ void compute_output(uint32_t off, const uint32_t* sm,
                     B1[i] = A1[i];
                 }
             }
-            const uint32_t cw = f2::kCoef[2 * kind + xi];
-            const int scale = (neg ? -1 : 1) * (dbl ? 2 : 1);
+            // coefficients in {-1, 0, 1}: bit 0 nonzero, bit 1 negative (4 bits per product)
+            const uint32_t cw = f2::kCoef[2 * kind + xi] ^ (neg ? 0x666666u : 0u);
             const uint32_t np = kind == f2::kKara ? 3u : 2u;
 #pragma unroll 1
             for (uint32_t j = 0; j < np; ++j) {
@@ -160,8 +172,9 @@ __device__ __forceinline__ void compute_output(uint32_t off, const uint32_t* sm,
                 }
                 uint32_t P[24];
                 f2::prod24(P, U, V);
-                f2::acc_add(acc[0], P, scale * sext4(cw >> (4 * j)));
-                f2::acc_add(acc[1], P, scale * sext4(cw >> (4 * (3 + j))));
+                const uint32_t ca = (cw >> (4 * j)) & 3u, cb = (cw >> (4 * (3 + j))) & 3u;
+                if (ca & 1u) f2::acc_add(acc[0], P, ca >> 1);
+                if (cb & 1u) f2::acc_add(acc[1], P, cb >> 1);
             }
         }
         uint32_t red[2][13];
