@@ -1,8 +1,12 @@
 """Generator of the Fp2-lane tower programs of the verify kernel (verify_fp2.cu).
 
-Execution model.  Six lanes own one pairing; lane k produces the k-th Fp2
+Execution model.  Twelve threads own one pairing, in two halves (two warps
+of a block); the thread pair (k, half 0) and (k, half 1) produces the k-th Fp2
 coefficient (tower order c0.c0, c0.c1, c0.c2, c1.c0, c1.c1, c1.c2) of each
-Fp12 result.  Every coefficient of every tower operation on the verify path
+Fp12 result.  The products of an output are split between the two halves;
+each half sums its share into both accumulators, the halves exchange one
+accumulator through shared memory, and half 0 reduces the real part, half 1
+the imaginary part.  Every coefficient of every tower operation on the verify path
 (gpu-crypto/cuda/field_sppark.cuh:52-197, gpu-crypto/cuda/api.cu:22-78) is
 written as one *output*:
 
@@ -189,6 +193,43 @@ def finish(o):
                 o.bias_lin_im = bk
             assert bk * P + poss < POST_LIMIT
     return o
+
+
+# ---------------------------------------------------------------- halves
+def split_halves(o):
+    """Assign the products of an output's terms to the two halves, balancing
+    their counts: whole terms first (largest first, to the lighter half), then
+    single products move from the heavier half while that narrows the gap.
+    Returns two lists of (term index, product mask)."""
+    load = [0, 0]
+    masks = [dict(), dict()]
+    for ti in sorted(range(len(o.terms)), key=lambda i: (-NPROD[o.terms[i].kind], i)):
+        n = NPROD[o.terms[ti].kind]
+        h = 0 if load[0] <= load[1] else 1
+        masks[h][ti] = (1 << n) - 1
+        load[h] += n
+    while abs(load[0] - load[1]) >= 2:
+        big = 0 if load[0] > load[1] else 1
+        ti = max(masks[big])
+        m = masks[big][ti]
+        bit = m.bit_length() - 1
+        masks[big][ti] = m & ~(1 << bit)
+        if not masks[big][ti]:
+            del masks[big][ti]
+        masks[1 - big][ti] = masks[1 - big].get(ti, 0) | (1 << bit)
+        load[big] -= 1
+        load[1 - big] += 1
+    halves = [sorted(masks[h].items()) for h in range(2)]
+    # every product exactly once
+    for ti, t in enumerate(o.terms):
+        m0 = dict(halves[0]).get(ti, 0)
+        m1 = dict(halves[1]).get(ti, 0)
+        assert m0 & m1 == 0 and (m0 | m1) == (1 << NPROD[t.kind]) - 1
+    return halves
+
+
+def half_products(o, h):
+    return sum(bin(m).count("1") for _, m in split_halves(o)[h]) if o.mode in (M_SIMPLE, M_FULL) else 0
 
 
 # ---------------------------------------------------------------- tower helpers
@@ -432,18 +473,26 @@ class Emulator:
         self.progs = {name: outs for name, outs, _ in progs}
 
     @staticmethod
-    def _acc(terms, slots, bases, bias_k):
-        acc = [bias_k[0] * P * R, bias_k[1] * P * R]
-        for t in terms:
-            X = slots[bases[t.x >> 4] + (t.x & 15)]
-            Y = slots[bases[t.y >> 4] + (t.y & 15)] if t.y is not None else None
-            al, be = t.coefs()
-            for k, (u, v) in enumerate(t.operands(X, Y)):
-                assert 0 <= u < R and 0 <= v < R
-                pr = u * v
-                acc[0] += al[k] * pr
-                acc[1] += be[k] * pr
-        return acc
+    def _acc(o, slots, bases):
+        """both halves' partial accumulators (half 0 holds the bias), summed
+        the way the device exchanges them"""
+        parts = []
+        for h, half in enumerate(split_halves(o)):
+            acc = [o.bias_re * P * R, o.bias_im * P * R] if h == 0 else [0, 0]
+            for ti, mask in half:
+                t = o.terms[ti]
+                X = slots[bases[t.x >> 4] + (t.x & 15)]
+                Y = slots[bases[t.y >> 4] + (t.y & 15)] if t.y is not None else None
+                al, be = t.coefs()
+                for k, (u, v) in enumerate(t.operands(X, Y)):
+                    if not (mask >> k) & 1:
+                        continue
+                    assert 0 <= u < R and 0 <= v < R
+                    pr = u * v
+                    acc[0] += al[k] * pr
+                    acc[1] += be[k] * pr
+            parts.append(acc)
+        return [parts[0][0] + parts[1][0], parts[0][1] + parts[1][1]]
 
     def run(self, name, slots, bases):
         outs = self.progs[name]
@@ -463,7 +512,7 @@ class Emulator:
                     v.append(qp(s))
                 v = tuple(v)
             else:
-                acc = self._acc(o.terms, slots, bases, (o.bias_re, o.bias_im))
+                acc = self._acc(o, slots, bases)
                 r = [redc(a) for a in acc]
                 if o.mode == M_SIMPLE:
                     v = (qp(r[0]), qp(r[1]))
@@ -517,21 +566,27 @@ def _limbs32(v, n=12):
 
 
 # ---------------------------------------------------------------- C emission
-def encode_term(t):
+def encode_term(t, mask):
     w = t.kind | (t.xi << 2) | ((1 if t.sign < 0 else 0) << 3) | (t.dbl << 4) | (t.yim << 5)
     w |= t.x << 8
     w |= (t.y if t.y is not None else 0) << 16
+    w |= mask << 24
     return w
 
 
-def encode_out(o):
-    """header: mode | nterms << 2 | nlin << 6 | dst << 8 | (c_re & 15) << 16 | (c_im & 15) << 20
-       biases: re | im << 8 | lin_re << 16 | lin_im << 24; then terms, then lins (coef & 15 | ref << 8)."""
-    nt, nl = len(o.terms), len(o.lins)
+def encode_out(o, h):
+    """The descriptor of half h of an output.
+       header: mode | nterms << 2 | nlin << 6 | dst << 8 | (c_re & 15) << 16 | (c_im & 15) << 20
+       biases: re | im << 8 | lin_re << 16 | lin_im << 24 (accumulator biases in half 0 only);
+       then terms (with the half's product mask in bits 24-26), then lins (coef & 15 | ref << 8)."""
+    half = split_halves(o)[h] if o.mode in (M_SIMPLE, M_FULL) else []
+    nt, nl = len(half), len(o.lins)
     assert nt < 16 and nl < 4
     hdr = o.mode | (nt << 2) | (nl << 6) | (o.dst << 8) | ((o.c_re & 15) << 16) | ((o.c_im & 15) << 20)
-    bias = o.bias_re | (o.bias_im << 8) | (o.bias_lin_re << 16) | (o.bias_lin_im << 24)
-    words = [hdr, bias] + [encode_term(t) for t in o.terms] + [(co & 15) | (r << 8) for co, r in o.lins]
+    bre, bim = (o.bias_re, o.bias_im) if h == 0 else (0, 0)
+    bias = bre | (bim << 8) | (o.bias_lin_re << 16) | (o.bias_lin_im << 24)
+    words = [hdr, bias] + [encode_term(o.terms[ti], m) for ti, m in half] + \
+        [(co & 15) | (r << 8) for co, r in o.lins]
     return words
 
 
@@ -550,23 +605,26 @@ def emit(path):
     words, index = [], []
     for n, outs, _ in progs:
         row = []
-        for o in outs:
-            if o is None:
-                row.append(0xffff)
-            else:
-                row.append(len(words))
-                words.extend(encode_out(o))
+        for h in range(2):
+            for o in outs:
+                if o is None:
+                    row.append(0xffff)
+                else:
+                    row.append(len(words))
+                    words.extend(encode_out(o, h))
+            row += [0xffff, 0xffff]
         index.append(row)
-    L.append("// per program and lane: first word of the lane's output descriptor (0xffff: none)")
-    L.append("__device__ __constant__ uint16_t kOutIndex[%d][8] = {" % len(progs))
+    L.append("// per program, half (8 entries each) and lane: first word of the output")
+    L.append("// descriptor (0xffff: none)")
+    L.append("__device__ __constant__ uint16_t kOutIndex[%d][16] = {" % len(progs))
     for (n, _, _), row in zip(progs, index):
-        L.append("    {%s, 0xffff, 0xffff},  // %s" % (", ".join("%d" % v for v in row), n))
+        L.append("    {%s},  // %s" % (", ".join("%d" % v for v in row), n))
     L.append("};")
     L.append("__device__ __constant__ uint32_t kDesc[%d] = {" % len(words))
     for i in range(0, len(words), 6):
         L.append("    " + ", ".join("0x%08xu" % w for w in words[i:i + 6]) + ",")
     L.append("};")
-    L.append("// accumulator coefficients per (kind, xi): alpha0..2, beta0..2 as 4-bit two's complement")
+    L.append("// accumulator coefficients per (kind, xi): alpha0..2, beta0..2, 4 bits each, in {-1, 0, 1}")
     L.append("__device__ __constant__ uint32_t kCoef[8] = {")
     row = []
     for kind in range(4):
@@ -604,15 +662,17 @@ def emit(path):
 def summary():
     out = []
     for n, outs, _ in build():
-        prods = []
+        per = []
         for o in outs:
-            if o is None or o.mode in (M_LIN, M_INVFP):
-                prods.append(0)
+            if o is None:
+                per.append((0, 0))
             else:
-                prods.append(sum(NPROD[t.kind] for t in o.terms))
+                per.append((half_products(o, 0), half_products(o, 1)))
+        mx = max(max(a, b) for a, b in per)
+        tot = sum(a + b for a, b in per)
         redcs = sum(2 for o in outs if o is not None and o.mode in (M_SIMPLE, M_FULL))
-        out.append("%-7s products per lane %s  (max %2d, total %3d), REDC %2d" % (n, prods, max(prods), sum(prods),
-                                                                                  redcs))
+        out.append("%-7s products per thread (half 0, half 1) %s  (max %2d, total %3d), REDC %2d"
+                   % (n, per, mx, tot, redcs))
     return out
 
 

@@ -1,8 +1,12 @@
-// Fp2-lane verify kernel: six lanes per verification, lane k producing the
-// k-th Fp2 coefficient of every Fp12 result from the generated descriptors
-// (fp2ops.inc, gen_fp2ops.py), with lazy reduction: all the Fp2 products that
-// feed one coefficient are summed exactly in two 832-bit accumulators and
-// reduced once.  Five verifications per warp (lanes 30 and 31 idle).
+// Fp2-lane verify kernel: twelve threads per verification in two halves (the
+// two warps of a block), thread (k, h) working on the k-th Fp2 coefficient of
+// every Fp12 result from the generated descriptors (fp2ops.inc,
+// gen_fp2ops.py), with lazy reduction: all the Fp2 products that feed one
+// coefficient are summed exactly in two 832-bit accumulators and reduced once.
+// The products of a coefficient are split between the halves; half h sums its
+// share, hands the other component's partial sum to its partner through
+// shared memory, and reduces component h (0: real, 1: imaginary).  Five
+// verifications per block (lanes 30 and 31 of each warp idle).
 //
 // Per verification (gpu-crypto/cuda/api.cu:80-91, api.cu:30-52, api.cu:65-78):
 //   Miller loop   for each of the 68 line coefficients: both pairs'
@@ -10,14 +14,16 @@
 //                 LINE1 and LINE2 multiply f by the two lines; 62 SQR in
 //                 between; CONJ at the end (x < 0)
 //   final exp     the reference's chain over 7 Fp12 groups, the inverse in 8
-//                 steps with an extended-Euclid Fp inverse on one lane
+//                 steps with an extended-Euclid Fp inverse on one thread
 //   result        canonical Gt compared with 1; optional Miller / Gt outputs
 //
 // Shared memory: 8 block-shared constant slots (0, 1, Frobenius constants),
 // then per pairing 7 groups of 6 Fp2 slots and a 12-slot C area (lines,
-// points).  An Fp2 slot is 24 words: re then im, each below 2^381 + p.  Every
-// program computes all outputs into registers, meets at __syncwarp, writes,
-// and meets again, so a program may overwrite its own inputs.
+// points), then the exchange area (per pairing and coefficient, one 26-word
+// partial sum per half) and per-pairing flags.  An Fp2 slot is 24 words: re
+// then im, each below 2^381 + p.  Every program accumulates, exchanges, meets,
+// reduces, meets, writes and meets again, so a program may overwrite its own
+// inputs.
 #include <cuda_runtime.h>
 
 #include "fp2ops.cuh"
@@ -29,19 +35,26 @@ namespace {
 
 constexpr uint64_t kXAbs = 0xd201000000010000ULL;
 constexpr int kLanes = 6;
-constexpr int kPairsPerWarp = 5;
+constexpr int kPairsPerBlock = 5;
+constexpr int kThreads = 64;                    // two halves of 32
 constexpr int kGroups = 7;
 constexpr int kTGroup = 3;                      // inversion temporaries: groups 3-5
 constexpr int kCOff = 6 * kGroups;              // C area after the groups
 constexpr int kPairSlots = kCOff + 12;          // Fp2 slots per pairing
 constexpr int kKSlots = f2::kKSlotCount;        // block-shared constants
 constexpr int kSlotWords = 24;
+constexpr int kSlotArea = (kKSlots + kPairsPerBlock * kPairSlots) * kSlotWords;  // words
+constexpr int kXchWords = 28;                   // 26 used; 112 B keeps uint4 alignment
+constexpr int kXchArea = kPairsPerBlock * kLanes * 2 * kXchWords;                 // words
+constexpr int kFlagArea = kPairsPerBlock * 2 + 2;                                // words
 
 struct Ctx {
-    uint32_t* sm;      // shared memory (words)
+    uint32_t* sm;      // shared memory (words): slots, then exchange, then flags
     uint32_t region;   // first slot of this pairing
-    int lane;          // 0..5 within the pairing; 6, 7 for the idle lanes 30, 31
-    bool active;       // lane belongs to a pairing
+    int pair;          // pairing within the block, 0..4 (5 for the idle lanes)
+    int lane;          // coefficient 0..5; 6, 7 for the idle lanes 30, 31
+    int half;          // warp of the block: 0 or 1
+    bool active;       // thread belongs to a pairing
 };
 
 struct Bases { uint32_t b[6]; };  // D, A, B, C, K, T: absolute slot of index 0
@@ -68,151 +81,185 @@ __device__ __forceinline__ void store_fp(uint32_t* sm, uint32_t slot, int comp, 
 
 __device__ __forceinline__ int sext4(uint32_t v) { return (int)(v << 28) >> 28; }
 
-// one output of a program: (re, im) into o0, o1
-__device__ __forceinline__ void compute_output(uint32_t off, const uint32_t* sm, const Bases& bs, uint32_t* o0,
-                                               uint32_t* o1) {
+// Phase 1 of an output (product modes): this half's products into both
+// accumulators, acc[1 - half] left in the exchange slot for the partner.
+__device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bases& bs, uint32_t* xch_out,
+                                           int half, uint32_t* own) {
+    const uint32_t hdr = f2::kDesc[off], bias = f2::kDesc[off + 1];
+    const uint32_t nt = (hdr >> 2) & 15u;
+    uint32_t acc[2][26];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+#pragma unroll
+        for (int i = 0; i < 12; ++i) acc[c][i] = 0;
+        acc[c][25] = 0;
+        f2::set_kp(acc[c] + 12, (bias >> (8 * c)) & 0xffu);
+    }
+    for (uint32_t t = 0; t < nt; ++t) {
+        const uint32_t w = f2::kDesc[off + 2 + t];
+        const uint32_t kind = w & 3u, xi = (w >> 2) & 1u, neg = (w >> 3) & 1u, dbl = (w >> 4) & 1u,
+                       yim = (w >> 5) & 1u, mask = (w >> 24) & 7u;
+        const uint32_t xs = slot_addr(bs, (w >> 8) & 0x7fu), ys = slot_addr(bs, (w >> 16) & 0x7fu);
+        // operands of products 0 and 1: (A0, B0), (A1, B1); KARA's product 2 is (A0 + A1, B0 + B1)
+        uint32_t A0[12], A1[12], B0[12], B1[12];
+        load_fp(A0, sm, xs, 0);
+        load_fp(A1, sm, xs, 1);
+        if (kind == f2::kKara) {
+            load_fp(B0, sm, ys, 0);
+            load_fp(B1, sm, ys, 1);
+            if (xi) {                       // X = xi X = (x0 - x1 + 3p, x0 + x1)
+                uint32_t s[12];
+                f2::add12(s, A0, A1);
+                f2::add3p_sub(A0, A0, A1);
+#pragma unroll
+                for (int i = 0; i < 12; ++i) A1[i] = s[i];
+            }
+            if (dbl) {
+                f2::dbl12(B0);
+                f2::dbl12(B1);
+            }
+        } else if (kind == f2::kSqr) {
+            f2::add3p_sub(B0, A0, A1);      // x0 - x1 + 3p
+#pragma unroll
+            for (int i = 0; i < 12; ++i) B1[i] = A1[i];
+            uint32_t s[12];
+            f2::add12(s, A0, A1);
+            f2::dbl12(A0);
+#pragma unroll
+            for (int i = 0; i < 12; ++i) {
+                A1[i] = A0[i];              // 2 x0
+                A0[i] = s[i];               // x0 + x1
+            }
+        } else if (kind == f2::kFpMul) {
+            load_fp(B0, sm, ys, yim);
+#pragma unroll
+            for (int i = 0; i < 12; ++i) B1[i] = B0[i];
+        } else {                            // NORM
+#pragma unroll
+            for (int i = 0; i < 12; ++i) {
+                B0[i] = A0[i];
+                B1[i] = A1[i];
+            }
+        }
+        // coefficients in {-1, 0, 1}: bit 0 nonzero, bit 1 negative (4 bits per product)
+        const uint32_t cw = f2::kCoef[2 * kind + xi] ^ (neg ? 0x666666u : 0u);
+        const uint32_t np = kind == f2::kKara ? 3u : 2u;
+#pragma unroll 1
+        for (uint32_t j = 0; j < np; ++j) {
+            if (!((mask >> j) & 1u)) continue;
+            uint32_t U[12], V[12];
+            if (j == 2) {
+                f2::add12(U, A0, A1);
+                f2::add12(V, B0, B1);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 12; ++i) {
+                    U[i] = j ? A1[i] : A0[i];
+                    V[i] = j ? B1[i] : B0[i];
+                }
+            }
+            uint32_t P[24];
+            f2::prod24(P, U, V);
+            const uint32_t ca = (cw >> (4 * j)) & 3u, cb = (cw >> (4 * (3 + j))) & 3u;
+            if (ca & 1u) f2::acc_add(acc[0], P, ca >> 1);
+            if (cb & 1u) f2::acc_add(acc[1], P, cb >> 1);
+        }
+    }
+    uint4* x = reinterpret_cast<uint4*>(xch_out);
+#pragma unroll
+    for (int i = 0; i < 24; i += 4)
+        x[i / 4] = half ? make_uint4(acc[0][i], acc[0][i + 1], acc[0][i + 2], acc[0][i + 3])
+                        : make_uint4(acc[1][i], acc[1][i + 1], acc[1][i + 2], acc[1][i + 3]);
+    xch_out[24] = half ? acc[0][24] : acc[1][24];
+    xch_out[25] = half ? acc[0][25] : acc[1][25];
+#pragma unroll
+    for (int i = 0; i < 26; ++i) own[i] = half ? acc[1][i] : acc[0][i];
+}
+
+// Phase 2: component `half` of the output into o (12 words).  own: this
+// half's accumulator of that component (product modes), xch_in: the partner's.
+__device__ __forceinline__ void finish(uint32_t off, const uint32_t* sm, const Bases& bs, int half, uint32_t* own,
+                                       const uint32_t* xch_in, uint32_t* o) {
     const uint32_t hdr = f2::kDesc[off], bias = f2::kDesc[off + 1];
     const uint32_t mode = hdr & 3u, nt = (hdr >> 2) & 15u, nl = (hdr >> 6) & 3u;
-    const int c_re = sext4(hdr >> 16), c_im = sext4(hdr >> 20);
+    const int cc = half ? sext4(hdr >> 20) : sext4(hdr >> 16);
+    const uint32_t bias_lin = (bias >> (16 + 8 * half)) & 0xffu;
     const uint32_t* lin = f2::kDesc + off + 2 + nt;
 
     if (mode == f2::kModeInvFp) {
-        fp z;
-        load_fp(z.w, sm, slot_addr(bs, lin[0] >> 8), 0);
-        fp r = f2::fp_inverse_mont(z);
+        if (half == 0) {
+            fp z;
+            load_fp(z.w, sm, slot_addr(bs, lin[0] >> 8), 0);
+            fp r = f2::fp_inverse_mont(z);
 #pragma unroll
-        for (int i = 0; i < 12; ++i) {
-            o0[i] = r.w[i];
-            o1[i] = 0;
+            for (int i = 0; i < 12; ++i) o[i] = r.w[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < 12; ++i) o[i] = 0;
         }
         return;
     }
-
-    uint32_t r[2][13];
+    uint32_t r[13];
     if (mode == f2::kModeLin) {
-        for (int c = 0; c < 2; ++c) {
-            f2::set_kp(r[c], (bias >> (16 + 8 * c)) & 0xffu);
-            const int cc = c ? c_im : c_re;
-            for (uint32_t j = 0; j < nl; ++j) {
-                uint32_t z[12];
-                load_fp(z, sm, slot_addr(bs, lin[j] >> 8), c);
-                f2::madd13(r[c], z, cc * sext4(lin[j]));
-            }
+        f2::set_kp(r, bias_lin);
+        for (uint32_t j = 0; j < nl; ++j) {
+            uint32_t z[12];
+            load_fp(z, sm, slot_addr(bs, lin[j] >> 8), half);
+            f2::madd13(r, z, cc * sext4(lin[j]));
         }
     } else {
-        uint32_t acc[2][26];
+        // own += partner's partial sum (26 limbs, modulo 2^832)
+        uint32_t p[26];
+        const uint4* x = reinterpret_cast<const uint4*>(xch_in);
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-#pragma unroll
-            for (int i = 0; i < 12; ++i) acc[c][i] = 0;
-            acc[c][25] = 0;
-            f2::set_kp(acc[c] + 12, (bias >> (8 * c)) & 0xffu);
+        for (int i = 0; i < 24; i += 4) {
+            const uint4 q = x[i / 4];
+            p[i] = q.x; p[i + 1] = q.y; p[i + 2] = q.z; p[i + 3] = q.w;
         }
-        for (uint32_t t = 0; t < nt; ++t) {
-            const uint32_t w = f2::kDesc[off + 2 + t];
-            const uint32_t kind = w & 3u, xi = (w >> 2) & 1u, neg = (w >> 3) & 1u, dbl = (w >> 4) & 1u,
-                           yim = (w >> 5) & 1u;
-            const uint32_t xs = slot_addr(bs, (w >> 8) & 0x7fu), ys = slot_addr(bs, (w >> 16) & 0x7fu);
-            // operands of products 0 and 1: (A0, B0), (A1, B1); KARA's product 2 is (A0 + A1, B0 + B1)
-            uint32_t A0[12], A1[12], B0[12], B1[12];
-            load_fp(A0, sm, xs, 0);
-            load_fp(A1, sm, xs, 1);
-            if (kind == f2::kKara) {
-                load_fp(B0, sm, ys, 0);
-                load_fp(B1, sm, ys, 1);
-                if (xi) {                       // X = xi X = (x0 - x1 + 3p, x0 + x1)
-                    uint32_t s[12];
-                    f2::add12(s, A0, A1);
-                    f2::add3p_sub(A0, A0, A1);
+        p[24] = xch_in[24];
+        p[25] = xch_in[25];
+        uint32_t c = 0;
 #pragma unroll
-                    for (int i = 0; i < 12; ++i) A1[i] = s[i];
-                }
-                if (dbl) {
-                    f2::dbl12(B0);
-                    f2::dbl12(B1);
-                }
-            } else if (kind == f2::kSqr) {
-                f2::add3p_sub(B0, A0, A1);      // x0 - x1 + 3p
-#pragma unroll
-                for (int i = 0; i < 12; ++i) B1[i] = A1[i];
-                uint32_t s[12];
-                f2::add12(s, A0, A1);
-                f2::dbl12(A0);
-#pragma unroll
-                for (int i = 0; i < 12; ++i) {
-                    A1[i] = A0[i];              // 2 x0
-                    A0[i] = s[i];               // x0 + x1
-                }
-            } else if (kind == f2::kFpMul) {
-                load_fp(B0, sm, ys, yim);
-#pragma unroll
-                for (int i = 0; i < 12; ++i) B1[i] = B0[i];
-            } else {                            // NORM
-#pragma unroll
-                for (int i = 0; i < 12; ++i) {
-                    B0[i] = A0[i];
-                    B1[i] = A1[i];
-                }
-            }
-            // coefficients in {-1, 0, 1}: bit 0 nonzero, bit 1 negative (4 bits per product)
-            const uint32_t cw = f2::kCoef[2 * kind + xi] ^ (neg ? 0x666666u : 0u);
-            const uint32_t np = kind == f2::kKara ? 3u : 2u;
-#pragma unroll 1
-            for (uint32_t j = 0; j < np; ++j) {
-                uint32_t U[12], V[12];
-                if (j == 2) {
-                    f2::add12(U, A0, A1);
-                    f2::add12(V, B0, B1);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 12; ++i) {
-                        U[i] = j ? A1[i] : A0[i];
-                        V[i] = j ? B1[i] : B0[i];
-                    }
-                }
-                uint32_t P[24];
-                f2::prod24(P, U, V);
-                const uint32_t ca = (cw >> (4 * j)) & 3u, cb = (cw >> (4 * (3 + j))) & 3u;
-                if (ca & 1u) f2::acc_add(acc[0], P, ca >> 1);
-                if (cb & 1u) f2::acc_add(acc[1], P, cb >> 1);
-            }
+        for (int i = 0; i < 26; ++i) {
+            const uint64_t s = (uint64_t)own[i] + p[i] + c;
+            own[i] = (uint32_t)s;
+            c = (uint32_t)(s >> 32);
         }
-        uint32_t red[2][13];
-        f2::redc26(red[0], acc[0]);
-        f2::redc26(red[1], acc[1]);
+        uint32_t red[13];
+        f2::redc26(red, own);
         if (mode == f2::kModeSimple) {
-            f2::qp_reduce(o0, red[0]);
-            f2::qp_reduce(o1, red[1]);
+            f2::qp_reduce(o, red);
             return;
         }
-        for (int c = 0; c < 2; ++c) {
-            uint32_t q[12];
-            f2::qp_reduce(q, red[c]);
-            f2::set_kp(r[c], (bias >> (16 + 8 * c)) & 0xffu);
-            f2::madd13(r[c], q, c ? c_im : c_re);
-            for (uint32_t j = 0; j < nl; ++j) {
-                uint32_t z[12];
-                load_fp(z, sm, slot_addr(bs, lin[j] >> 8), c);
-                f2::madd13(r[c], z, sext4(lin[j]));
-            }
+        uint32_t q[12];
+        f2::qp_reduce(q, red);
+        f2::set_kp(r, bias_lin);
+        f2::madd13(r, q, cc);
+        for (uint32_t j = 0; j < nl; ++j) {
+            uint32_t z[12];
+            load_fp(z, sm, slot_addr(bs, lin[j] >> 8), half);
+            f2::madd13(r, z, sext4(lin[j]));
         }
     }
-    f2::qp_reduce(o0, r[0]);
-    f2::qp_reduce(o1, r[1]);
+    f2::qp_reduce(o, r);
 }
 
-// run program `pid` on the pairing: compute, meet, write, meet
-static __device__ __noinline__ void run(int pid, const Ctx& c, Bases bs) {
-    const uint32_t off = c.active ? f2::kOutIndex[pid][c.lane] : 0xffffu;
-    uint32_t o0[12], o1[12];
-    if (off != 0xffffu) compute_output(off, c.sm, bs, o0, o1);
-    __syncwarp();
-    if (off != 0xffffu) {
-        const uint32_t dst = slot_addr(bs, (f2::kDesc[off] >> 8) & 0x7fu);
-        store_fp(c.sm, dst, 0, o0);
-        store_fp(c.sm, dst, 1, o1);
-    }
-    __syncwarp();
+// run program `pid` on the pairing: accumulate, exchange, meet, reduce, meet,
+// write, meet.  Every thread of the block takes part in every barrier.
+static __device__ __noinline__ void run(int pid, uint32_t* sm, int pair, int lane, int half, Bases bs) {
+    const bool active = pair < kPairsPerBlock;
+    const uint32_t off = active ? f2::kOutIndex[pid][8 * half + lane] : 0xffffu;
+    const uint32_t mode = off != 0xffffu ? (f2::kDesc[off] & 3u) : 0u;
+    const bool prod = off != 0xffffu && (mode == f2::kModeSimple || mode == f2::kModeFull);
+    uint32_t* xch = sm + kSlotArea + ((active ? pair : 0) * kLanes + (active ? lane % kLanes : 0)) * 2 * kXchWords;
+    uint32_t own[26];
+    if (prod) accumulate(off, sm, bs, xch + kXchWords * half, half, own);
+    __syncthreads();
+    uint32_t o[12];
+    if (off != 0xffffu) finish(off, sm, bs, half, own, xch + kXchWords * (1 - half), o);
+    __syncthreads();
+    if (off != 0xffffu) store_fp(sm, slot_addr(bs, (f2::kDesc[off] >> 8) & 0x7fu), half, o);
+    __syncthreads();
 }
 
 __device__ __forceinline__ void call(const Ctx& c, int pid, int d, int a = 0, int b = 0) {
@@ -223,7 +270,7 @@ __device__ __forceinline__ void call(const Ctx& c, int pid, int d, int a = 0, in
     bs.b[3] = c.region + kCOff;
     bs.b[4] = 0;
     bs.b[5] = grp(c, kTGroup);
-    run(pid, c, bs);
+    run(pid, c.sm, c.pair, c.lane, c.half, bs);
 }
 
 __device__ __forceinline__ void inverse(const Ctx& c, int d, int a) {
@@ -238,9 +285,9 @@ __device__ __forceinline__ void copy_fp_from_global(uint32_t* sm, uint32_t slot,
     d[2] = __ldg(s + 2);
 }
 
-// line coefficient `ci` of both pairs into the C area (lane k: pair k / 3,
-// coefficient k % 3), then LSCALE.  A skipped pair gets the line (0, 0, 1),
-// which leaves f unchanged.
+// line coefficient `ci` of both pairs into the C area (thread (k, h): pair
+// k / 3, coefficient k % 3, component h), then LSCALE.  A skipped pair gets
+// the line (0, 0, 1), which leaves f unchanged.
 __device__ __forceinline__ void load_lines(const Ctx& c, const uint64_t* q1, bool skip1, const uint64_t* q2,
                                            bool skip2, int ci) {
     if (c.active) {
@@ -249,15 +296,13 @@ __device__ __forceinline__ void load_lines(const Ctx& c, const uint64_t* q1, boo
         const bool skip = pair ? skip2 : skip1;
         const uint32_t slot = c.region + kCOff + 6 * pair + k;
         if (skip) {
-            fp v = k == 2 ? fp_one() : fp_zero();
-            store_fp(c.sm, slot, 0, v.w);
-            store_fp(c.sm, slot, 1, fp_zero().w);
+            fp v = (k == 2 && c.half == 0) ? fp_one() : fp_zero();
+            store_fp(c.sm, slot, c.half, v.w);
         } else {
-            copy_fp_from_global(c.sm, slot, 0, q + 36 * ci + 12 * k);
-            copy_fp_from_global(c.sm, slot, 1, q + 36 * ci + 12 * k + 6);
+            copy_fp_from_global(c.sm, slot, c.half, q + 36 * ci + 12 * k + 6 * c.half);
         }
     }
-    __syncwarp();
+    __syncthreads();
     call(c, f2::P_LSCALE, 0);
 }
 
@@ -331,35 +376,33 @@ __device__ __forceinline__ fp canonical(fp v) {
     return v;
 }
 
-// canonical group `g` -> out (72 u64) and the "is one" test over the pairing's lanes
+// canonical group `g` -> out (72 u64) and the "is one" test over the
+// pairing's twelve threads (a flag per pairing and half in shared memory)
 __device__ __forceinline__ bool emit_group(const Ctx& c, int g, uint64_t* out) {
     bool ok = true;
     if (c.active) {
-        fp re, im;
-        load_fp(re.w, c.sm, grp(c, g) + c.lane, 0);
-        load_fp(im.w, c.sm, grp(c, g) + c.lane, 1);
-        re = canonical(re);
-        im = canonical(im);
-        if (out) {
-            fp_store_u64(out + 12 * c.lane, re);
-            fp_store_u64(out + 12 * c.lane + 6, im);
-        }
-        ok = (c.lane == 0 ? fp_eq(re, fp_one()) : fp_is_zero(re)) && fp_is_zero(im);
+        fp v;
+        load_fp(v.w, c.sm, grp(c, g) + c.lane, c.half);
+        v = canonical(v);
+        if (out) fp_store_u64(out + 12 * c.lane + 6 * c.half, v);
+        ok = (c.lane == 0 && c.half == 0) ? fp_eq(v, fp_one()) : fp_is_zero(v);
     }
     const unsigned bad = __ballot_sync(0xffffffffu, !ok);
-    const unsigned lane32 = threadIdx.x & 31u;
-    const unsigned first = lane32 - (unsigned)c.lane;
-    const unsigned mask = c.active ? (0x3fu << first) : 0u;
-    return (bad & mask) == 0;
+    uint32_t* flags = c.sm + kSlotArea + kXchArea;
+    if (c.active && c.lane == 0) {
+        const unsigned first = (threadIdx.x & 31u);
+        flags[2 * c.pair + c.half] = (bad >> first) & 0x3fu;
+    }
+    __syncthreads();
+    const bool one = c.active && (flags[2 * c.pair] | flags[2 * c.pair + 1]) == 0;
+    __syncthreads();
+    return one;
 }
 
-constexpr int kWarpsPerBlock = 1;
-
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_verify_fp2(VerifyArgs a, const uint32_t* __restrict__ in_status) {
+__global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const uint32_t* __restrict__ in_status) {
     extern __shared__ uint4 smem4[];
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem4);
-    const int warps = blockDim.x >> 5;
-    const int warp = threadIdx.x >> 5, lane32 = threadIdx.x & 31;
+    const int half = threadIdx.x >> 5, lane32 = threadIdx.x & 31;
     const int pi = lane32 / kLanes;
 
     for (int i = threadIdx.x; i < kKSlots * kSlotWords; i += blockDim.x) sm[i] = f2::kKSlots[i / kSlotWords][i % kSlotWords];
@@ -367,18 +410,22 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_verify_fp2(VerifyArgs a
 
     Ctx c;
     c.sm = sm;
-    c.active = pi < kPairsPerWarp;
+    c.active = pi < kPairsPerBlock;
+    c.pair = pi;
+    c.half = half;
     c.lane = c.active ? lane32 % kLanes : 6 + (lane32 & 1);
-    c.region = kKSlots + (warp * kPairsPerWarp + (c.active ? pi : 0)) * kPairSlots;
+    c.region = kKSlots + (c.active ? pi : 0) * kPairSlots;
+    uint32_t* bcast = sm + kSlotArea + kXchArea + 2 * kPairsPerBlock;
 
-    int next = (blockIdx.x * warps + warp) * kPairsPerWarp;
-    const int stride = gridDim.x * warps * kPairsPerWarp;
+    int next = blockIdx.x * kPairsPerBlock;
+    const int stride = gridDim.x * kPairsPerBlock;
     for (;;) {
         int base;
         if (a.work_counter) {
-            int b = 0;
-            if (lane32 == 0) b = atomicAdd(a.work_counter, kPairsPerWarp);
-            base = __shfl_sync(0xffffffffu, b, 0);
+            if (threadIdx.x == 0) bcast[0] = (uint32_t)atomicAdd(a.work_counter, kPairsPerBlock);
+            __syncthreads();
+            base = (int)bcast[0];
+            __syncthreads();
         } else {
             base = next;
             next += stride;
@@ -399,14 +446,14 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_verify_fp2(VerifyArgs a
             pk = a.pk_tables + kCoeffU64 * pki;
             skip1 = g1_limbs_identity(sx, sy) || status != 0;
             skip2 = g1_limbs_identity(hx, hy) || (a.pk_identity && a.pk_identity[pki]) || status != 0;
-            if (c.lane == 0) {
+            if (c.lane == 0 && c.half == 0) {
                 const uint32_t C = c.region + kCOff;
                 store_fp(sm, C + 0 * 6 + 3, 0, skip1 ? fp_zero().w : sx.w);
                 store_fp(sm, C + 0 * 6 + 3, 1, skip1 ? fp_zero().w : sy.w);
                 store_fp(sm, C + 1 * 6 + 3, 0, skip2 ? fp_zero().w : hx.w);
                 store_fp(sm, C + 1 * 6 + 3, 1, skip2 ? fp_zero().w : hy.w);
             }
-        } else if (c.active && c.lane == 0) {
+        } else if (c.active && c.lane == 0 && c.half == 0) {
             const uint32_t C = c.region + kCOff;
             for (int pair = 0; pair < 2; ++pair) {
                 store_fp(sm, C + pair * 6 + 3, 0, fp_zero().w);
@@ -414,11 +461,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_verify_fp2(VerifyArgs a
             }
         }
         // f = 1
-        if (c.active) {
-            store_fp(sm, grp(c, 0) + c.lane, 0, c.lane == 0 ? fp_one().w : fp_zero().w);
-            store_fp(sm, grp(c, 0) + c.lane, 1, fp_zero().w);
-        }
-        __syncwarp();
+        if (c.active) store_fp(sm, grp(c, 0) + c.lane, c.half, (c.lane == 0 && c.half == 0) ? fp_one().w : fp_zero().w);
+        __syncthreads();
 
         // Miller loop over |x| >> 1 below its leading bit (api.cu:30-52)
         int ci = 0;
@@ -433,14 +477,12 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_verify_fp2(VerifyArgs a
 
         final_exp(c);
         const bool one = emit_group(c, 0, (have && a.gt_out) ? a.gt_out + 72 * (size_t)item : nullptr);
-        if (have && c.lane == 0) a.results[item] = status != 0 ? -status : (one ? 1 : 0);
-        __syncwarp();
+        if (have && c.lane == 0 && c.half == 0) a.results[item] = status != 0 ? -status : (one ? 1 : 0);
+        __syncthreads();
     }
 }
 
-size_t smem_bytes() {
-    return (size_t)(kKSlots + kWarpsPerBlock * kPairsPerWarp * kPairSlots) * kSlotWords * 4;
-}
+size_t smem_bytes() { return (size_t)(kSlotArea + kXchArea + kFlagArea) * 4; }
 
 cudaError_t configure() {
     static cudaError_t done =
@@ -451,8 +493,7 @@ cudaError_t configure() {
 int resident() {
     if (configure() != cudaSuccess) return 0;
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_verify_fp2, 32 * kWarpsPerBlock, smem_bytes()) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_verify_fp2, kThreads, smem_bytes()) != cudaSuccess)
         return 0;
     return blocks;
 }
@@ -468,15 +509,14 @@ cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, in
     if (a.n <= 0) return cudaSuccess;
     cudaError_t e = configure();
     if (e != cudaSuccess) return e;
-    const int per_block = kWarpsPerBlock * kPairsPerWarp;
-    const int need = (a.n + per_block - 1) / per_block;
+    const int need = (a.n + kPairsPerBlock - 1) / kPairsPerBlock;
     const int res = resident();
     const int per_sm = blocks_per_sm > 0 ? blocks_per_sm : (res > 0 ? res : 1);
     const int cap = per_sm * sms;
     int blocks = a.work_counter ? cap : (need < cap || blocks_per_sm <= 0 ? need : cap);
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
-    k_verify_fp2<<<blocks, 32 * kWarpsPerBlock, smem_bytes(), s>>>(a, in_status);
+    k_verify_fp2<<<blocks, kThreads, smem_bytes(), s>>>(a, in_status);
     return cudaGetLastError();
 }
 
