@@ -11,60 +11,107 @@ namespace f2 {
 
 // p[0..23] = a * b, schoolbook rows with the CIOS carry chains of fp.cuh.
 // After row i the partial product is below 2^(384 + 32 (i + 1)), so the hi
-// chain never carries out of p[i + 12].
+// chain never carries out of p[i + 12].  Row 0 writes p[0..12] outright.
 __device__ __forceinline__ void prod24(uint32_t* p, const uint32_t* a, const uint32_t* b) {
+    // row 0 writes p[0..12] without reading it: lo products, then the hi chain
 #pragma unroll
-    for (int i = 0; i < 24; ++i) p[i] = 0;
+    for (int j = 0; j < 12; ++j) p[j] = a[j] * b[0];
+    asm("mad.hi.cc.u32 %0, %12, %24, %0;\n\t"
+        "madc.hi.cc.u32 %1, %13, %24, %1;\n\t"
+        "madc.hi.cc.u32 %2, %14, %24, %2;\n\t"
+        "madc.hi.cc.u32 %3, %15, %24, %3;\n\t"
+        "madc.hi.cc.u32 %4, %16, %24, %4;\n\t"
+        "madc.hi.cc.u32 %5, %17, %24, %5;\n\t"
+        "madc.hi.cc.u32 %6, %18, %24, %6;\n\t"
+        "madc.hi.cc.u32 %7, %19, %24, %7;\n\t"
+        "madc.hi.cc.u32 %8, %20, %24, %8;\n\t"
+        "madc.hi.cc.u32 %9, %21, %24, %9;\n\t"
+        "madc.hi.cc.u32 %10, %22, %24, %10;\n\t"
+        "madc.hi.u32 %11, %23, %24, 0;"
+        : "+r"(p[1]), "+r"(p[2]), "+r"(p[3]), "+r"(p[4]), "+r"(p[5]), "+r"(p[6]), "+r"(p[7]), "+r"(p[8]),
+          "+r"(p[9]), "+r"(p[10]), "+r"(p[11]), "=r"(p[12])
+        : BLS_A12(a), "r"(b[0]));
 #pragma unroll
-    for (int i = 0; i < 12; ++i) {
+    for (int i = 13; i < 24; ++i) p[i] = 0;
+#pragma unroll
+    for (int i = 1; i < 12; ++i) {
         chain_lo(p + i, a, b[i]);
         chain_hi(p + i, a, b[i]);
     }
 }
 
-// acc[0..25] += p (neg = 0) or -= p (neg = 1), modulo 2^832: the operand is
-// p complemented for a subtraction, with the complement's +1 as the first carry.
-__device__ __forceinline__ void acc_add(uint32_t* acc, const uint32_t* p, uint32_t neg) {
-    const uint32_t m = 0u - neg;
-    uint32_t v[24];
-#pragma unroll
-    for (int i = 0; i < 24; ++i) v[i] = p[i] ^ m;
-    uint32_t dummy;
-    asm("add.cc.u32 %26, %27, 0xffffffff;\n\t"
-        "addc.cc.u32 %0, %0, %28;\n\t"
-        "addc.cc.u32 %1, %1, %29;\n\t"
-        "addc.cc.u32 %2, %2, %30;\n\t"
-        "addc.cc.u32 %3, %3, %31;\n\t"
-        "addc.cc.u32 %4, %4, %32;\n\t"
-        "addc.cc.u32 %5, %5, %33;\n\t"
-        "addc.cc.u32 %6, %6, %34;\n\t"
-        "addc.cc.u32 %7, %7, %35;\n\t"
-        "addc.cc.u32 %8, %8, %36;\n\t"
-        "addc.cc.u32 %9, %9, %37;\n\t"
-        "addc.cc.u32 %10, %10, %38;\n\t"
-        "addc.cc.u32 %11, %11, %39;\n\t"
-        "addc.cc.u32 %12, %12, %40;\n\t"
-        "addc.cc.u32 %13, %13, %41;\n\t"
-        "addc.cc.u32 %14, %14, %42;\n\t"
-        "addc.cc.u32 %15, %15, %43;\n\t"
-        "addc.cc.u32 %16, %16, %44;\n\t"
-        "addc.cc.u32 %17, %17, %45;\n\t"
-        "addc.cc.u32 %18, %18, %46;\n\t"
-        "addc.cc.u32 %19, %19, %47;\n\t"
-        "addc.cc.u32 %20, %20, %48;\n\t"
-        "addc.cc.u32 %21, %21, %49;\n\t"
-        "addc.cc.u32 %22, %22, %50;\n\t"
-        "addc.cc.u32 %23, %23, %51;\n\t"
-        "addc.cc.u32 %24, %24, %52;\n\t"
-        "addc.u32 %25, %25, %52;"
+// acc[0..25] -= p (24 limbs), modulo 2^832
+__device__ __forceinline__ void acc_sub(uint32_t* acc, const uint32_t* p) {
+    asm("sub.cc.u32 %0, %0, %26;\n\t"
+        "subc.cc.u32 %1, %1, %27;\n\t"
+        "subc.cc.u32 %2, %2, %28;\n\t"
+        "subc.cc.u32 %3, %3, %29;\n\t"
+        "subc.cc.u32 %4, %4, %30;\n\t"
+        "subc.cc.u32 %5, %5, %31;\n\t"
+        "subc.cc.u32 %6, %6, %32;\n\t"
+        "subc.cc.u32 %7, %7, %33;\n\t"
+        "subc.cc.u32 %8, %8, %34;\n\t"
+        "subc.cc.u32 %9, %9, %35;\n\t"
+        "subc.cc.u32 %10, %10, %36;\n\t"
+        "subc.cc.u32 %11, %11, %37;\n\t"
+        "subc.cc.u32 %12, %12, %38;\n\t"
+        "subc.cc.u32 %13, %13, %39;\n\t"
+        "subc.cc.u32 %14, %14, %40;\n\t"
+        "subc.cc.u32 %15, %15, %41;\n\t"
+        "subc.cc.u32 %16, %16, %42;\n\t"
+        "subc.cc.u32 %17, %17, %43;\n\t"
+        "subc.cc.u32 %18, %18, %44;\n\t"
+        "subc.cc.u32 %19, %19, %45;\n\t"
+        "subc.cc.u32 %20, %20, %46;\n\t"
+        "subc.cc.u32 %21, %21, %47;\n\t"
+        "subc.cc.u32 %22, %22, %48;\n\t"
+        "subc.cc.u32 %23, %23, %49;\n\t"
+        "subc.cc.u32 %24, %24, 0;\n\t"
+        "subc.u32 %25, %25, 0;"
         : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3]), "+r"(acc[4]), "+r"(acc[5]), "+r"(acc[6]),
           "+r"(acc[7]), "+r"(acc[8]), "+r"(acc[9]), "+r"(acc[10]), "+r"(acc[11]), "+r"(acc[12]), "+r"(acc[13]),
           "+r"(acc[14]), "+r"(acc[15]), "+r"(acc[16]), "+r"(acc[17]), "+r"(acc[18]), "+r"(acc[19]),
-          "+r"(acc[20]), "+r"(acc[21]), "+r"(acc[22]), "+r"(acc[23]), "+r"(acc[24]), "+r"(acc[25]), "=r"(dummy)
-        : "r"(neg), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
-          "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]),
-          "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]),
-          "r"(m));
+          "+r"(acc[20]), "+r"(acc[21]), "+r"(acc[22]), "+r"(acc[23]), "+r"(acc[24]), "+r"(acc[25])
+        : "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]), "r"(p[8]),
+          "r"(p[9]), "r"(p[10]), "r"(p[11]), "r"(p[12]), "r"(p[13]), "r"(p[14]), "r"(p[15]), "r"(p[16]),
+          "r"(p[17]), "r"(p[18]), "r"(p[19]), "r"(p[20]), "r"(p[21]), "r"(p[22]), "r"(p[23]));
+}
+
+// acc[0..25] += p (24 limbs), modulo 2^832
+__device__ __forceinline__ void acc_plus(uint32_t* acc, const uint32_t* p) {
+    asm("add.cc.u32 %0, %0, %26;\n\t"
+        "addc.cc.u32 %1, %1, %27;\n\t"
+        "addc.cc.u32 %2, %2, %28;\n\t"
+        "addc.cc.u32 %3, %3, %29;\n\t"
+        "addc.cc.u32 %4, %4, %30;\n\t"
+        "addc.cc.u32 %5, %5, %31;\n\t"
+        "addc.cc.u32 %6, %6, %32;\n\t"
+        "addc.cc.u32 %7, %7, %33;\n\t"
+        "addc.cc.u32 %8, %8, %34;\n\t"
+        "addc.cc.u32 %9, %9, %35;\n\t"
+        "addc.cc.u32 %10, %10, %36;\n\t"
+        "addc.cc.u32 %11, %11, %37;\n\t"
+        "addc.cc.u32 %12, %12, %38;\n\t"
+        "addc.cc.u32 %13, %13, %39;\n\t"
+        "addc.cc.u32 %14, %14, %40;\n\t"
+        "addc.cc.u32 %15, %15, %41;\n\t"
+        "addc.cc.u32 %16, %16, %42;\n\t"
+        "addc.cc.u32 %17, %17, %43;\n\t"
+        "addc.cc.u32 %18, %18, %44;\n\t"
+        "addc.cc.u32 %19, %19, %45;\n\t"
+        "addc.cc.u32 %20, %20, %46;\n\t"
+        "addc.cc.u32 %21, %21, %47;\n\t"
+        "addc.cc.u32 %22, %22, %48;\n\t"
+        "addc.cc.u32 %23, %23, %49;\n\t"
+        "addc.cc.u32 %24, %24, 0;\n\t"
+        "addc.u32 %25, %25, 0;"
+        : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3]), "+r"(acc[4]), "+r"(acc[5]), "+r"(acc[6]),
+          "+r"(acc[7]), "+r"(acc[8]), "+r"(acc[9]), "+r"(acc[10]), "+r"(acc[11]), "+r"(acc[12]), "+r"(acc[13]),
+          "+r"(acc[14]), "+r"(acc[15]), "+r"(acc[16]), "+r"(acc[17]), "+r"(acc[18]), "+r"(acc[19]),
+          "+r"(acc[20]), "+r"(acc[21]), "+r"(acc[22]), "+r"(acc[23]), "+r"(acc[24]), "+r"(acc[25])
+        : "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]), "r"(p[8]),
+          "r"(p[9]), "r"(p[10]), "r"(p[11]), "r"(p[12]), "r"(p[13]), "r"(p[14]), "r"(p[15]), "r"(p[16]),
+          "r"(p[17]), "r"(p[18]), "r"(p[19]), "r"(p[20]), "r"(p[21]), "r"(p[22]), "r"(p[23]));
 }
 
 // x = 2 x (12 limbs; x below 2^383)

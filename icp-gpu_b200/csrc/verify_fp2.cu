@@ -161,8 +161,14 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
             uint32_t P[24];
             f2::prod24(P, U, V);
             const uint32_t ca = (cw >> (4 * j)) & 3u, cb = (cw >> (4 * (3 + j))) & 3u;
-            if (ca & 1u) f2::acc_add(acc[0], P, ca >> 1);
-            if (cb & 1u) f2::acc_add(acc[1], P, cb >> 1);
+            if (ca & 1u) {
+                if (ca >> 1) f2::acc_sub(acc[0], P);
+                else f2::acc_plus(acc[0], P);
+            }
+            if (cb & 1u) {
+                if (cb >> 1) f2::acc_sub(acc[1], P);
+                else f2::acc_plus(acc[1], P);
+            }
         }
     }
     uint4* x = reinterpret_cast<uint4*>(xch_out);
