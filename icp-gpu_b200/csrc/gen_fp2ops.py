@@ -432,6 +432,80 @@ PROGRAMS = [
 ]
 
 
+# ---------------------------------------------------------------- driver sequence
+# The verify kernel runs one op sequence per verification (api.cu:30-52 Miller
+# loop, api.cu:54-78 final exponentiation).  An op is a program on Fp12 groups
+# (D, A, B), LOAD_LINES(ci) (both pairs' coefficient ci into the C area) or
+# MILLER_DONE (the Miller value is complete in group 0).
+X_ABS = 0xd201000000010000
+OP_MILLER_DONE, OP_LOAD_LINES = 30, 31
+T_GROUP = 3       # the inverse's temporaries use groups 3-5 from slot 0
+
+
+def driver_sequence():
+    pid = {name: i for i, (name, _, _) in enumerate(PROGRAMS)}
+    seq = []
+
+    def prog(name, d, a=0, b=0):
+        seq.append((pid[name], d, a, b, 0))
+
+    def lines(ci):
+        seq.append((OP_LOAD_LINES, 0, 0, 0, ci))
+        prog("LSCALE", 0)
+        prog("LINE1", 0, 0)
+        prog("LINE2", 0, 0)
+
+    ci = 0
+    for bit in range(61, -1, -1):
+        lines(ci)
+        ci += 1
+        if ((X_ABS >> 1) >> bit) & 1:
+            lines(ci)
+            ci += 1
+        prog("SQR", 0, 0)
+    lines(ci)
+    prog("CONJ", 0, 0)
+    seq.append((OP_MILLER_DONE, 0, 0, 0, 0))
+
+    def inv(d, a):
+        for k in range(1, 9):
+            prog("INV%d" % k, d, a)
+
+    def cyc_exp(dst, x, spare):
+        prog("COPY", dst, x)
+        cur, oth = dst, spare
+        for i in range(62, -1, -1):
+            prog("CYCSQR", cur, cur)
+            if (X_ABS >> i) & 1:
+                prog("MUL", oth, cur, x)
+                cur, oth = oth, cur
+        prog("CONJ", dst, cur)
+
+    # final exponentiation of group 0 into group 0: the reference's chain,
+    # api.cu:65-78, over seven groups
+    prog("CONJ", 1, 0); inv(2, 0); prog("MUL", 3, 1, 2); prog("FROB", 0, 3); prog("FROB", 1, 0)
+    prog("MUL", 2, 1, 3); prog("COPY", 0, 2); prog("CYCSQR", 0, 0); prog("CONJ", 0, 0)
+    cyc_exp(1, 2, 3)
+    prog("MUL", 3, 0, 1)
+    cyc_exp(0, 3, 4)
+    prog("CONJ", 3, 3); prog("MUL", 4, 2, 3); prog("COPY", 3, 1); prog("CYCSQR", 3, 3)
+    cyc_exp(5, 0, 6)
+    prog("MUL", 6, 1, 5); prog("FROB", 1, 6); prog("FROB", 6, 1); prog("MUL", 1, 4, 6)
+    cyc_exp(4, 5, 6)
+    prog("MUL", 5, 3, 4)
+    cyc_exp(3, 5, 4)
+    prog("MUL", 4, 1, 3); prog("CONJ", 1, 2); prog("MUL", 3, 5, 1); prog("MUL", 1, 2, 0)
+    prog("FROB", 0, 1); prog("FROB", 2, 0); prog("FROB", 0, 2); prog("MUL", 1, 4, 0); prog("FROB", 2, 3)
+    prog("MUL", 0, 1, 2)
+    return seq
+
+
+def encode_op(op):
+    code, d, a, b, ci = op
+    assert code < 32 and d < 8 and a < 8 and b < 8 and ci < 128
+    return code | (d << 5) | (a << 8) | (b << 11) | (ci << 14)
+
+
 def build():
     progs = []
     for name, fn, doc in PROGRAMS:
@@ -649,6 +723,17 @@ def emit(path):
     L.append("__device__ __constant__ uint32_t kR3[12] = {" + ", ".join(_limbs32(R * R * R % P)) + "};")
     L.append("// 3p, the offset of SQR's x0 - x1 + 3p")
     L.append("__device__ __constant__ uint32_t k3P[12] = {" + ", ".join(_limbs32(K3P)) + "};")
+    seq = driver_sequence()
+    L.append("// the verify op sequence: code | D << 5 | A << 8 | B << 11 | ci << 14; code < kNumPrograms is")
+    L.append("// a program, kOpLoadLines loads line coefficient ci, kOpMillerDone marks the Miller value")
+    L.append("constexpr uint32_t kOpMillerDone = %d, kOpLoadLines = %d;" % (OP_MILLER_DONE, OP_LOAD_LINES))
+    L.append("constexpr int kTGroup = %d;" % T_GROUP)
+    L.append("constexpr int kSeqLen = %d;" % len(seq))
+    L.append("__device__ __constant__ uint32_t kSeq[%d] = {" % len(seq))
+    words = [encode_op(op) for op in seq]
+    for i in range(0, len(words), 8):
+        L.append("    " + ", ".join("0x%05xu" % w for w in words[i:i + 8]) + ",")
+    L.append("};")
     L.append("// QP[h] = floor(h * 2^381 / p) * p, 13 words padded to 16")
     L.append("__device__ const uint32_t kQP2[128][16] = {")
     for q in QP:

@@ -33,12 +33,10 @@
 namespace bls {
 namespace {
 
-constexpr uint64_t kXAbs = 0xd201000000010000ULL;
 constexpr int kLanes = 6;
 constexpr int kPairsPerBlock = 5;
 constexpr int kThreads = 64;                    // two halves of 32
 constexpr int kGroups = 7;
-constexpr int kTGroup = 3;                      // inversion temporaries: groups 3-5
 constexpr int kCOff = 6 * kGroups;              // C area after the groups
 constexpr int kPairSlots = kCOff + 12;          // Fp2 slots per pairing
 constexpr int kKSlots = f2::kKSlotCount;        // block-shared constants
@@ -251,8 +249,9 @@ __device__ __forceinline__ void finish(uint32_t off, const uint32_t* sm, const B
 }
 
 // run program `pid` on the pairing: accumulate, exchange, meet, reduce, meet,
-// write, meet.  Every thread of the block takes part in every barrier.
-static __device__ __noinline__ void run(int pid, uint32_t* sm, int pair, int lane, int half, Bases bs) {
+// write, meet.  Every thread of the block takes part in every barrier.  It has
+// one call site (the op loop of the kernel), so it is inlined there.
+__device__ __forceinline__ void run(int pid, uint32_t* sm, int pair, int lane, int half, const Bases& bs) {
     const bool active = pair < kPairsPerBlock;
     const uint32_t off = active ? f2::kOutIndex[pid][8 * half + lane] : 0xffffu;
     const uint32_t mode = off != 0xffffu ? (f2::kDesc[off] & 3u) : 0u;
@@ -268,21 +267,6 @@ static __device__ __noinline__ void run(int pid, uint32_t* sm, int pair, int lan
     __syncthreads();
 }
 
-__device__ __forceinline__ void call(const Ctx& c, int pid, int d, int a = 0, int b = 0) {
-    Bases bs;
-    bs.b[0] = grp(c, d);
-    bs.b[1] = grp(c, a);
-    bs.b[2] = grp(c, b);
-    bs.b[3] = c.region + kCOff;
-    bs.b[4] = 0;
-    bs.b[5] = grp(c, kTGroup);
-    run(pid, c.sm, c.pair, c.lane, c.half, bs);
-}
-
-__device__ __forceinline__ void inverse(const Ctx& c, int d, int a) {
-    for (int k = f2::P_INV1; k <= f2::P_INV8; ++k) call(c, k, d, a);
-}
-
 __device__ __forceinline__ void copy_fp_from_global(uint32_t* sm, uint32_t slot, int comp, const uint64_t* src) {
     const uint4* s = reinterpret_cast<const uint4*>(src);
     uint4* d = reinterpret_cast<uint4*>(sm + kSlotWords * slot + 12 * comp);
@@ -292,8 +276,8 @@ __device__ __forceinline__ void copy_fp_from_global(uint32_t* sm, uint32_t slot,
 }
 
 // line coefficient `ci` of both pairs into the C area (thread (k, h): pair
-// k / 3, coefficient k % 3, component h), then LSCALE.  A skipped pair gets
-// the line (0, 0, 1), which leaves f unchanged.
+// k / 3, coefficient k % 3, component h).  A skipped pair gets the line
+// (0, 0, 1), which leaves f unchanged.
 __device__ __forceinline__ void load_lines(const Ctx& c, const uint64_t* q1, bool skip1, const uint64_t* q2,
                                            bool skip2, int ci) {
     if (c.active) {
@@ -309,65 +293,6 @@ __device__ __forceinline__ void load_lines(const Ctx& c, const uint64_t* q1, boo
         }
     }
     __syncthreads();
-    call(c, f2::P_LSCALE, 0);
-}
-
-__device__ __forceinline__ void line_step(const Ctx& c, const uint64_t* q1, bool skip1, const uint64_t* q2,
-                                          bool skip2, int ci) {
-    load_lines(c, q1, skip1, q2, skip2, ci);
-    call(c, f2::P_LINE1, 0, 0);
-    call(c, f2::P_LINE2, 0, 0);
-}
-
-__device__ __forceinline__ void cyc_exp(const Ctx& c, int dst, int x, int spare) {
-    call(c, f2::P_COPY, dst, x);
-    int cur = dst, oth = spare;
-    for (int i = 62; i >= 0; --i) {
-        call(c, f2::P_CYCSQR, cur, cur);
-        if ((kXAbs >> i) & 1) {
-            call(c, f2::P_MUL, oth, cur, x);
-            int t = cur; cur = oth; oth = t;
-        }
-    }
-    call(c, f2::P_CONJ, dst, cur);
-}
-
-// final exponentiation of group 0 into group 0 (api.cu:65-78)
-__device__ __forceinline__ void final_exp(const Ctx& c) {
-    call(c, f2::P_CONJ, 1, 0);       // t0 = conj(f)            G1
-    inverse(c, 2, 0);                // t1 = f^-1               G2
-    call(c, f2::P_MUL, 3, 1, 2);     // t2 = t0 t1              G3
-    call(c, f2::P_FROB, 0, 3);
-    call(c, f2::P_FROB, 1, 0);       // frob^2(t2)              G1
-    call(c, f2::P_MUL, 2, 1, 3);     // t2 = frob^2(t2) t2      G2 (f = t2)
-    call(c, f2::P_COPY, 0, 2);
-    call(c, f2::P_CYCSQR, 0, 0);
-    call(c, f2::P_CONJ, 0, 0);       // t1 = conj(cyc_sqr(t2))  G0
-    cyc_exp(c, 1, 2, 3);             // t3 = cyc_exp(t2)        G1
-    call(c, f2::P_MUL, 3, 0, 1);     // t4 = t1 t3              G3
-    cyc_exp(c, 0, 3, 4);             // t1 = cyc_exp(t4)        G0
-    call(c, f2::P_CONJ, 3, 3);       // t4 = conj(t4)
-    call(c, f2::P_MUL, 4, 2, 3);     // f = f t4                G4
-    call(c, f2::P_COPY, 3, 1);
-    call(c, f2::P_CYCSQR, 3, 3);     // t4 = cyc_sqr(t3)        G3
-    cyc_exp(c, 5, 0, 6);             // t0 = cyc_exp(t1)        G5
-    call(c, f2::P_MUL, 6, 1, 5);     // t3 = t3 t0              G6
-    call(c, f2::P_FROB, 1, 6);
-    call(c, f2::P_FROB, 6, 1);       // t3 = frob^2(t3)         G6
-    call(c, f2::P_MUL, 1, 4, 6);     // f = f t3                G1
-    cyc_exp(c, 4, 5, 6);             // c = cyc_exp(t0)         G4
-    call(c, f2::P_MUL, 5, 3, 4);     // t4 = t4 c               G5
-    cyc_exp(c, 3, 5, 4);             // c = cyc_exp(t4)         G3
-    call(c, f2::P_MUL, 4, 1, 3);     // f = f c                 G4
-    call(c, f2::P_CONJ, 1, 2);       // conj(t2)                G1
-    call(c, f2::P_MUL, 3, 5, 1);     // t4 = t4 conj(t2)        G3
-    call(c, f2::P_MUL, 1, 2, 0);     // t2 = t2 t1              G1
-    call(c, f2::P_FROB, 0, 1);
-    call(c, f2::P_FROB, 2, 0);
-    call(c, f2::P_FROB, 0, 2);       // t2 = frob^3(t2)         G0
-    call(c, f2::P_MUL, 1, 4, 0);     // f = f t2                G1
-    call(c, f2::P_FROB, 2, 3);       // t4 = frob(t4)           G2
-    call(c, f2::P_MUL, 0, 1, 2);     // f = f t4                G0
 }
 
 // canonical form of a slot value (below 2^381 + p < 3p)
@@ -470,18 +395,26 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
         if (c.active) store_fp(sm, grp(c, 0) + c.lane, c.half, (c.lane == 0 && c.half == 0) ? fp_one().w : fp_zero().w);
         __syncthreads();
 
-        // Miller loop over |x| >> 1 below its leading bit (api.cu:30-52)
-        int ci = 0;
-        for (int b = 61; b >= 0; --b) {
-            line_step(c, a.g2, skip1, pk, skip2, ci++);
-            if (((kXAbs >> 1) >> b) & 1) line_step(c, a.g2, skip1, pk, skip2, ci++);
-            call(c, f2::P_SQR, 0, 0);
+        // the op sequence: Miller loop over |x| >> 1 below its leading bit
+        // (api.cu:30-52), then the final exponentiation (api.cu:65-78)
+        for (int s = 0; s < f2::kSeqLen; ++s) {
+            const uint32_t e = f2::kSeq[s];
+            const uint32_t code = e & 31u;
+            if (code == f2::kOpLoadLines) {
+                load_lines(c, a.g2, skip1, pk, skip2, (int)(e >> 14));
+            } else if (code == f2::kOpMillerDone) {
+                if (a.ml_out) emit_group(c, 0, have ? a.ml_out + 72 * (size_t)item : nullptr);
+            } else {
+                Bases bs;
+                bs.b[0] = grp(c, (e >> 5) & 7u);
+                bs.b[1] = grp(c, (e >> 8) & 7u);
+                bs.b[2] = grp(c, (e >> 11) & 7u);
+                bs.b[3] = c.region + kCOff;
+                bs.b[4] = 0;
+                bs.b[5] = grp(c, f2::kTGroup);
+                run((int)code, sm, c.pair, c.lane, c.half, bs);
+            }
         }
-        line_step(c, a.g2, skip1, pk, skip2, ci);
-        call(c, f2::P_CONJ, 0, 0);
-        if (a.ml_out) emit_group(c, 0, have ? a.ml_out + 72 * (size_t)item : nullptr);
-
-        final_exp(c);
         const bool one = emit_group(c, 0, (have && a.gt_out) ? a.gt_out + 72 * (size_t)item : nullptr);
         if (have && c.lane == 0 && c.half == 0) a.results[item] = status != 0 ? -status : (one ? 1 : 0);
         __syncthreads();

@@ -11,10 +11,10 @@ import gen_fp2ops as G  # noqa: E402
 
 import bls_ref as B  # noqa: E402
 
-X_ABS = 0xD201000000010000
+
 K_SLOTS = 8
 GROUPS = 7
-T_GROUP = 3          # inversion temporaries start at group 3 (13 slots)
+T_GROUP = G.T_GROUP  # inversion temporaries start at group 3 (13 slots)
 C_OFF = 6 * GROUPS   # C area after the groups
 
 
@@ -68,34 +68,6 @@ class Machine:
         return out
 
 
-def cyc_exp(m, dst, x, spare):
-    m.call("COPY", dst, x)
-    cur, oth = dst, spare
-    for i in range(62, -1, -1):
-        m.call("CYCSQR", cur, cur)
-        if (X_ABS >> i) & 1:
-            m.call("MUL", oth, cur, x)
-            cur, oth = oth, cur
-    m.call("CONJ", dst, cur)
-
-
-def final_exp(m):
-    c = m.call
-    c("CONJ", 1, 0); m.inv(2, 0); c("MUL", 3, 1, 2); c("FROB", 0, 3); c("FROB", 1, 0); c("MUL", 2, 1, 3)
-    c("COPY", 0, 2); c("CYCSQR", 0, 0); c("CONJ", 0, 0)
-    cyc_exp(m, 1, 2, 3)
-    c("MUL", 3, 0, 1)
-    cyc_exp(m, 0, 3, 4)
-    c("CONJ", 3, 3); c("MUL", 4, 2, 3); c("COPY", 3, 1); c("CYCSQR", 3, 3)
-    cyc_exp(m, 5, 0, 6)
-    c("MUL", 6, 1, 5); c("FROB", 1, 6); c("FROB", 6, 1); c("MUL", 1, 4, 6)
-    cyc_exp(m, 4, 5, 6)
-    c("MUL", 5, 3, 4)
-    cyc_exp(m, 3, 5, 4)
-    c("MUL", 4, 1, 3); c("CONJ", 1, 2); c("MUL", 3, 5, 1); c("MUL", 1, 2, 0)
-    c("FROB", 0, 1); c("FROB", 2, 0); c("FROB", 0, 2); c("MUL", 1, 4, 0); c("FROB", 2, 3); c("MUL", 0, 1, 2)
-
-
 def verify(sig, nhm, g2_limbs, pk_limbs, skip1=False, skip2=False):
     """sig / nhm: canonical affine points; tables: 2448 u64.  Returns
     (miller, gt) as canonical flat Fp lists (normal form)."""
@@ -116,24 +88,15 @@ def verify(sig, nhm, g2_limbs, pk_limbs, skip1=False, skip2=False):
                     w = [int(x) for x in tab[36 * ci + 12 * k: 36 * ci + 12 * k + 12]]
                     v = (sum(x << (64 * i) for i, x in enumerate(w[:6])), sum(x << (64 * i) for i, x in enumerate(w[6:])))
                 m.slots[C + 6 * pair + k] = v
-        m.call("LSCALE", 0)
 
-    def lines():
-        m.call("LINE1", 0, 0)
-        m.call("LINE2", 0, 0)
-
-    ci = 0
-    for b in range(61, -1, -1):
-        load(ci); ci += 1
-        lines()
-        if ((X_ABS >> 1) >> b) & 1:
-            load(ci); ci += 1
-            lines()
-        m.call("SQR", 0, 0)
-    load(ci)
-    lines()
-    m.call("CONJ", 0, 0)
-    ml = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]
-    final_exp(m)
+    names = [name for name, _, _ in G.PROGRAMS]
+    ml = None
+    for code, d, a, b, ci in G.driver_sequence():
+        if code == G.OP_LOAD_LINES:
+            load(ci)
+        elif code == G.OP_MILLER_DONE:
+            ml = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]
+        else:
+            m.call(names[code], d, a, b)
     gt = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]
     return ml, gt
