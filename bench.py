@@ -119,6 +119,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": samples}
 
 
+def max_over_ranks(pg, value, device):
+    """the largest `value` over all ranks (every rank gets it); `pg` is
+    torch.distributed or None for one process"""
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(items_per_rank, world, steps, seconds):
+    """verifies/s of the whole job: every rank verifies its own shard each step,
+    and the job takes as long as its slowest rank"""
+    return items_per_rank * world * steps / seconds
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -268,14 +285,10 @@ def run_gpu(args):
     if pg:
         pg.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if pg:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(pg, sum(step_ms), dev)
     res = d_res.cpu().numpy()
     assert (res == wl["expect"]).all(), "GPU accept bits differ from the expected ones (timed run)"
-    value = N_ITEMS * world * args.steps / (total_ms / 1e3)
+    value = whole_job_rate(N_ITEMS, world, args.steps, total_ms / 1e3)
     kernel_ms = statistics.mean(step_ms)
 
     # e2e through the C ABI from host buffers
@@ -290,12 +303,8 @@ def run_gpu(args):
         if k >= args.warmup:
             e2e_times.append(dt)
     assert (r == wl["expect"]).all()
-    e2e_s = sum(e2e_times)
-    if pg:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = N_ITEMS * world * args.steps / e2e_s
+    e2e_s = max_over_ranks(pg, sum(e2e_times), dev)
+    e2e_value = whole_job_rate(N_ITEMS, world, args.steps, e2e_s)
 
     batching = serving = None
     if not args.no_extras:
