@@ -91,6 +91,31 @@ struct bls_ctx {
     uint8_t* d_pk_inf = nullptr;    // max_pks
     int n_pks = 0;
     std::vector<uint8_t> h_pk_inf;
+    // the same tables with every row divided by its c2, and their Miller
+    // correction factors (the Fp2-lane kernel's normalised lines)
+    uint64_t* d_g2_norm = nullptr;  // 2448
+    uint64_t* d_pk_norm = nullptr;  // max_pks x 2448
+    uint64_t* d_corr = nullptr;     // (1 + max_pks) x 12: generator, then keys
+    uint8_t* d_norm_bad = nullptr;  // (1 + max_pks): a table with a zero c2
+    bool norm_ok = true;            // every table normalised
+
+    // normalise table `src` into `dst`, correction factor into slot `k` of d_corr
+    int normalize(const uint64_t* src, uint64_t* dst, int k) {
+        CK(bls::launch_lines_normalize(src, 1, dst, d_corr + 12 * (size_t)k, d_norm_bad + k, stream));
+        uint8_t bad = 0;
+        CK(cudaMemcpyAsync(&bad, d_norm_bad + k, 1, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (bad) norm_ok = false;
+        return BLS_OK;
+    }
+    // normalised-line arguments of a verify over the registered tables
+    void set_norm(bls::VerifyArgs& a) const {
+        if (!norm_ok) return;
+        a.g2_norm = d_g2_norm;
+        a.pk_norm = d_pk_norm;
+        a.g2_corr = d_corr;
+        a.pk_corr = d_corr + 12;
+    }
 
     int grow(DevBuf& b, size_t bytes) {
         if (bytes <= b.cap) return BLS_OK;
@@ -136,6 +161,8 @@ struct bls_ctx {
         if (d_g2) cudaFree(d_g2);
         if (d_pk) cudaFree(d_pk);
         if (d_pk_inf) cudaFree(d_pk_inf);
+        for (void* q : {(void*)d_g2_norm, (void*)d_pk_norm, (void*)d_corr, (void*)d_norm_bad})
+            if (q) cudaFree(q);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -159,13 +186,18 @@ int ctx_init(bls_ctx* c, const bls_config* cfg) {
     CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     size_t pk_bytes = (size_t)c->cfg.max_pks * bls::kCoeffU64 * 8;
-    size_t need = pk_bytes + c->cfg.max_pks + bls::kCoeffU64 * 8 + 24 * 8;
+    size_t norm_bytes = pk_bytes + bls::kCoeffU64 * 8 + (size_t)(c->cfg.max_pks + 1) * (12 * 8 + 1);
+    size_t need = pk_bytes + c->cfg.max_pks + bls::kCoeffU64 * 8 + 24 * 8 + norm_bytes;
     if (c->cfg.mem_cap_bytes && need > c->cfg.mem_cap_bytes)
         return fail(BLS_ERR_NOMEM, "pk tables (%zu bytes) exceed the device budget", need);
     CK(cudaMalloc(&c->d_pk, pk_bytes));
     CK(cudaMalloc(&c->d_pk_inf, c->cfg.max_pks));
     CK(cudaMalloc(&c->d_g2, bls::kCoeffU64 * 8));
-    c->dev_bytes = pk_bytes + c->cfg.max_pks + bls::kCoeffU64 * 8;
+    CK(cudaMalloc(&c->d_pk_norm, pk_bytes));
+    CK(cudaMalloc(&c->d_g2_norm, bls::kCoeffU64 * 8));
+    CK(cudaMalloc(&c->d_corr, (size_t)(c->cfg.max_pks + 1) * 12 * 8));
+    CK(cudaMalloc(&c->d_norm_bad, c->cfg.max_pks + 1));
+    c->dev_bytes = pk_bytes + c->cfg.max_pks + bls::kCoeffU64 * 8 + norm_bytes;
     c->h_pk_inf.assign(c->cfg.max_pks, 0);
     CK(cudaMemsetAsync(c->d_pk_inf, 0, c->cfg.max_pks, c->stream));
     // generator line table, computed on the device
@@ -175,7 +207,7 @@ int ctx_init(bls_ctx* c, const bls_config* cfg) {
     CK(bls::launch_g2_prepare(d_q, 1, c->d_g2, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaFree(d_q));
-    return BLS_OK;
+    return c->normalize(c->d_g2, c->d_g2_norm, 0);
 }
 
 // default context behind the reference ABI (device 0, as the reference selects)
@@ -254,6 +286,7 @@ int enqueue(bls_ctx* c, size_t n, int fmt, bool persistent, bool want_ml, bool w
     a.nhms = (const uint64_t*)c->d_nhms.p;
     a.g2 = c->d_g2;
     a.pk_tables = c->d_pk;
+    c->set_norm(a);
     a.pk_index = (const int32_t*)c->d_pkidx.p;
     a.pk_identity = c->d_pk_inf;
     a.n = (int)n;
@@ -278,8 +311,10 @@ int check_ids(bls_ctx* c, const int32_t* ids, int n) {
 namespace bls {
 CtxView ctx_view(bls_ctx* c) {
     std::lock_guard<std::mutex> lk(c->mu);
+    bls::VerifyArgs a{};
+    c->set_norm(a);
     return CtxView{c->cfg.device, c->sms, c->cfg.lanes_per_pairing, c->cfg.blocks_per_sm,
-                   c->d_g2, c->d_pk, c->d_pk_inf, c->n_pks};
+                   c->d_g2, c->d_pk, c->d_pk_inf, c->n_pks, a.g2_norm, a.pk_norm, a.g2_corr, a.pk_corr};
 }
 }  // namespace bls
 
@@ -341,7 +376,9 @@ int bls_pk_register_coeffs(bls_ctx* ctx, const uint64_t* coeffs, int is_identity
     uint8_t inf = is_identity ? 1 : 0;
     ctx->h_pk_inf[id] = inf;
     CK(cudaMemcpyAsync(ctx->d_pk_inf + id, &ctx->h_pk_inf[id], 1, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    int nrc = ctx->normalize(ctx->d_pk + (size_t)id * bls::kCoeffU64, ctx->d_pk_norm + (size_t)id * bls::kCoeffU64,
+                             1 + id);
+    if (nrc) return nrc;
     ctx->n_pks++;
     *pk_id = id;
     return BLS_OK;
@@ -360,7 +397,9 @@ int bls_pk_register_affine(bls_ctx* ctx, const uint64_t* q24, int32_t* pk_id) {
                               ctx->stream));
     ctx->h_pk_inf[id] = 0;
     CK(cudaMemcpyAsync(ctx->d_pk_inf + id, &ctx->h_pk_inf[id], 1, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    int nrc = ctx->normalize(ctx->d_pk + (size_t)id * bls::kCoeffU64, ctx->d_pk_norm + (size_t)id * bls::kCoeffU64,
+                             1 + id);
+    if (nrc) return nrc;
     ctx->n_pks++;
     *pk_id = id;
     return BLS_OK;
@@ -516,6 +555,7 @@ int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* 
         a.nhms = b->neg_hms;
         a.g2 = ctx->d_g2;
         a.pk_tables = ctx->d_pk;
+        ctx->set_norm(a);
         a.pk_index = b->pk_ids;
         a.pk_identity = ctx->d_pk_inf;
         a.n = b->n;
@@ -563,6 +603,7 @@ int bls_verify_batch_device(bls_ctx* ctx, const bls_batch* b, int32_t* results_d
     a.nhms = b->neg_hms;
     a.g2 = ctx->d_g2;
     a.pk_tables = ctx->d_pk;
+    ctx->set_norm(a);
     a.pk_index = b->pk_ids;
     a.pk_identity = ctx->d_pk_inf;
     a.n = b->n;

@@ -40,6 +40,17 @@ __device__ __forceinline__ void prod24(uint32_t* p, const uint32_t* a, const uin
     }
 }
 
+// acc[12..25] += x (neg = 0) or -= x (neg = 1): acc += +-x 2^384, modulo 2^832
+__device__ __forceinline__ void acc_add_hi(uint32_t* acc, const uint32_t* x, uint32_t neg) {
+    uint32_t c = neg, m = 0u - neg;
+#pragma unroll
+    for (int i = 0; i < 14; ++i) {
+        const uint64_t s = (uint64_t)acc[12 + i] + ((i < 12 ? x[i] : 0u) ^ m) + c;
+        acc[12 + i] = (uint32_t)s;
+        c = (uint32_t)(s >> 32);
+    }
+}
+
 // acc[0..25] -= p (24 limbs), modulo 2^832
 __device__ __forceinline__ void acc_sub(uint32_t* acc, const uint32_t* p) {
     asm("sub.cc.u32 %0, %0, %26;\n\t"

@@ -74,7 +74,7 @@ K_FROB = 2     # 2..6: conj(k1), conj(k2), conj(k12), conj(k1 k12), conj(k2 k12)
 C_C0, C_C1, C_C2, C_PT, C_L2, C_L3 = range(6)
 
 # ---------------------------------------------------------------- kinds
-KARA, SQR, FPMUL, NORM = range(4)
+KARA, SQR, FPMUL, NORM, ONE = range(5)
 # (alpha, beta) per product, plain and times xi
 COEF = {
     (KARA, 0): ((1, -1, 0), (-1, -1, 1)),
@@ -85,7 +85,7 @@ COEF = {
     (FPMUL, 1): ((1, -1), (1, 1)),
     (NORM, 0): ((1, 1), (0, 0)),
 }
-NPROD = {KARA: 3, SQR: 2, FPMUL: 2, NORM: 2}
+NPROD = {KARA: 3, SQR: 2, FPMUL: 2, NORM: 2, ONE: 1}
 M_SIMPLE, M_FULL, M_LIN, M_INVFP = range(4)
 
 
@@ -94,18 +94,23 @@ class Term:
 
     def __init__(self, kind, x, y=None, xi=0, sign=1, dbl=0, yim=0):
         self.kind, self.x, self.y, self.xi, self.sign, self.dbl, self.yim = kind, x, y, xi, sign, dbl, yim
-        if kind in (SQR, NORM):
+        if kind in (SQR, NORM, ONE):
             self.y = x
         assert not (kind == NORM and xi)
         assert not (dbl and kind != KARA)
 
     def coefs(self):
+        if self.kind == ONE:
+            return [self.sign], [self.sign]
         a, b = COEF[(self.kind, self.xi)]
         return [self.sign * v for v in a], [self.sign * v for v in b]
 
     def operands(self, X, Y):
-        """(U, V) integer pairs for the products, from component values."""
+        """(U, V) integer pairs for the products, from component values.  A ONE
+        term is X itself, placed in the high half of the accumulators (X R)."""
         x0, x1 = X
+        if self.kind == ONE:
+            return [(x0, x1)]
         if self.kind == KARA:
             if self.xi:
                 x0, x1 = x0 - x1 + K3P, x0 + x1
@@ -140,10 +145,14 @@ def _operand_bounds(t):
         return [(bx0, by), (bx1, by), (bx0 + bx1, 2 * by)]
     if t.kind == SQR:
         return [(2 * B, B + K3P), (2 * B, B)]
+    if t.kind == ONE:
+        return [(B, B)]
     return [(B, B), (B, B)]
 
 
 def _prod_bounds(t):
+    if t.kind == ONE:
+        return [SLOT_BOUND * R]
     out = []
     for bu, bv in _operand_bounds(t):
         assert bu <= R and bv <= R, "operand bound"
@@ -285,6 +294,31 @@ def prog_line(pair):
             terms.append(Term(KARA, ref(B_A, T_OF_W[i]), lr, xi=int(k - j < 0)))
         outs.append(finish(Out(ref(B_D, t), terms=terms)))
     return outs
+
+
+def prog_line_norm(pair):
+    """D = A * (1 + l2 w^2 + l3 w^3): the line of prog_line divided by its c2
+    (tables normalised once per key; the Miller value differs from the
+    reference's by an Fp2 factor that the final exponentiation removes and
+    that SCALE1 / SCALE2 multiply back when the Miller value is wanted)."""
+    o = 6 * pair
+    lref = {2: ref(B_C, o + C_L2), 3: ref(B_C, o + C_L3)}
+    outs = []
+    for t in range(6):
+        k = W_OF_T[t]
+        terms = [Term(ONE, ref(B_A, t))]
+        for j, lr in sorted(lref.items()):
+            i = (k - j) % 6
+            terms.append(Term(KARA, ref(B_A, T_OF_W[i]), lr, xi=int(k - j < 0)))
+        outs.append(finish(Out(ref(B_D, t), terms=terms)))
+    return outs
+
+
+def prog_scale(pair):
+    """D = A * s, s the Fp2 in the C area's c2 slot of `pair` (a key's Miller
+    correction factor)"""
+    s_ref = ref(B_C, 6 * pair + C_C2)
+    return [finish(Out(ref(B_D, t), terms=[Term(KARA, ref(B_A, t), s_ref)])) for t in range(6)]
 
 
 def prog_lscale():
@@ -429,6 +463,10 @@ PROGRAMS = [
     ("INV6", prog_inv6, "T9 = T6^-1"),
     ("INV7", prog_inv7, "T10-12 = Fp6 inverse"),
     ("INV8", prog_inv8, "D = A^-1"),
+    ("LINE1N", lambda: prog_line_norm(0), "D = A * normalised line of pair 1"),
+    ("LINE2N", lambda: prog_line_norm(1), "D = A * normalised line of pair 2"),
+    ("SCALE1", lambda: prog_scale(0), "D = A * (Miller correction of pair 1)"),
+    ("SCALE2", lambda: prog_scale(1), "D = A * (Miller correction of pair 2)"),
 ]
 
 
@@ -438,13 +476,17 @@ PROGRAMS = [
 # (D, A, B), LOAD_LINES(ci) (both pairs' coefficient ci into the C area) or
 # MILLER_DONE (the Miller value is complete in group 0).
 X_ABS = 0xd201000000010000
-OP_MILLER_DONE, OP_LOAD_LINES = 30, 31
+OP_LOAD_CORR, OP_MILLER_DONE, OP_LOAD_LINES = 29, 30, 31
+COND_ML = 1 << 21     # op runs only when the Miller value is wanted
 T_GROUP = 3       # the inverse's temporaries use groups 3-5 from slot 0
 
 
-def driver_sequence():
+def driver_sequence(normalised=False):
+    """The op sequence of one verification; `normalised`: the line tables are
+    divided by their c2 (LINE1N / LINE2N)."""
     pid = {name: i for i, (name, _, _) in enumerate(PROGRAMS)}
     seq = []
+    l1, l2 = ("LINE1N", "LINE2N") if normalised else ("LINE1", "LINE2")
 
     def prog(name, d, a=0, b=0):
         seq.append((pid[name], d, a, b, 0))
@@ -452,8 +494,8 @@ def driver_sequence():
     def lines(ci):
         seq.append((OP_LOAD_LINES, 0, 0, 0, ci))
         prog("LSCALE", 0)
-        prog("LINE1", 0, 0)
-        prog("LINE2", 0, 0)
+        prog(l1, 0, 0)
+        prog(l2, 0, 0)
 
     ci = 0
     for bit in range(61, -1, -1):
@@ -465,7 +507,14 @@ def driver_sequence():
         prog("SQR", 0, 0)
     lines(ci)
     prog("CONJ", 0, 0)
-    seq.append((OP_MILLER_DONE, 0, 0, 0, 0))
+    if normalised:
+        # Miller value = f * (generator's correction) * (key's correction), into group 1
+        seq.append((OP_LOAD_CORR | COND_ML, 0, 0, 0, 0))
+        seq.append((pid["SCALE1"] | COND_ML, 1, 0, 0, 0))
+        seq.append((pid["SCALE2"] | COND_ML, 1, 1, 0, 0))
+        seq.append((OP_MILLER_DONE, 1, 0, 0, 0))
+    else:
+        seq.append((OP_MILLER_DONE, 0, 0, 0, 0))
 
     def inv(d, a):
         for k in range(1, 9):
@@ -502,8 +551,10 @@ def driver_sequence():
 
 def encode_op(op):
     code, d, a, b, ci = op
+    cond = code & COND_ML
+    code &= ~COND_ML
     assert code < 32 and d < 8 and a < 8 and b < 8 and ci < 128
-    return code | (d << 5) | (a << 8) | (b << 11) | (ci << 14)
+    return code | (d << 5) | (a << 8) | (b << 11) | (ci << 14) | cond
 
 
 def build():
@@ -558,6 +609,11 @@ class Emulator:
                 X = slots[bases[t.x >> 4] + (t.x & 15)]
                 Y = slots[bases[t.y >> 4] + (t.y & 15)] if t.y is not None else None
                 al, be = t.coefs()
+                if t.kind == ONE:
+                    if mask & 1:
+                        acc[0] += al[0] * X[0] * R
+                        acc[1] += be[0] * X[1] * R
+                    continue
                 for k, (u, v) in enumerate(t.operands(X, Y)):
                     if not (mask >> k) & 1:
                         continue
@@ -641,7 +697,7 @@ def _limbs32(v, n=12):
 
 # ---------------------------------------------------------------- C emission
 def encode_term(t, mask):
-    w = t.kind | (t.xi << 2) | ((1 if t.sign < 0 else 0) << 3) | (t.dbl << 4) | (t.yim << 5)
+    w = t.kind | (t.xi << 3) | ((1 if t.sign < 0 else 0) << 4) | (t.dbl << 5) | (t.yim << 6)
     w |= t.x << 8
     w |= (t.y if t.y is not None else 0) << 16
     w |= mask << 24
@@ -674,7 +730,8 @@ def emit(path):
     L.append("constexpr int kNumPrograms = %d;" % len(progs))
     L.append("constexpr uint32_t kModeSimple = %d, kModeFull = %d, kModeLin = %d, kModeInvFp = %d;"
              % (M_SIMPLE, M_FULL, M_LIN, M_INVFP))
-    L.append("constexpr uint32_t kKara = %d, kSqr = %d, kFpMul = %d, kNorm = %d;" % (KARA, SQR, FPMUL, NORM))
+    L.append("constexpr uint32_t kKara = %d, kSqr = %d, kFpMul = %d, kNorm = %d, kOne = %d;"
+             % (KARA, SQR, FPMUL, NORM, ONE))
     L += ["constexpr int kKFrob = %d;" % K_FROB, ""]
     words, index = [], []
     for n, outs, _ in progs:
@@ -699,9 +756,9 @@ def emit(path):
         L.append("    " + ", ".join("0x%08xu" % w for w in words[i:i + 6]) + ",")
     L.append("};")
     L.append("// accumulator coefficients per (kind, xi): alpha0..2, beta0..2, 4 bits each, in {-1, 0, 1}")
-    L.append("__device__ __constant__ uint32_t kCoef[8] = {")
+    L.append("__device__ __constant__ uint32_t kCoef[10] = {")
     row = []
-    for kind in range(4):
+    for kind in range(5):
         for xi in range(2):
             al, be = COEF.get((kind, xi), ((0, 0, 0), (0, 0, 0)))
             al, be = list(al) + [0] * (3 - len(al)), list(be) + [0] * (3 - len(be))
@@ -723,16 +780,24 @@ def emit(path):
     L.append("__device__ __constant__ uint32_t kR3[12] = {" + ", ".join(_limbs32(R * R * R % P)) + "};")
     L.append("// 3p, the offset of SQR's x0 - x1 + 3p")
     L.append("__device__ __constant__ uint32_t k3P[12] = {" + ", ".join(_limbs32(K3P)) + "};")
-    seq = driver_sequence()
-    L.append("// the verify op sequence: code | D << 5 | A << 8 | B << 11 | ci << 14; code < kNumPrograms is")
-    L.append("// a program, kOpLoadLines loads line coefficient ci, kOpMillerDone marks the Miller value")
-    L.append("constexpr uint32_t kOpMillerDone = %d, kOpLoadLines = %d;" % (OP_MILLER_DONE, OP_LOAD_LINES))
+    L.append("// the verify op sequences (raw and normalised line tables): code | D << 5 | A << 8 | B << 11 |")
+    L.append("// ci << 14; code < kNumPrograms is a program, kOpLoadLines loads line coefficient ci,")
+    L.append("// kOpMillerDone marks the Miller value")
+    L.append("// kOpLoadCorr loads the Miller correction factors; ops with kCondMl run only when the Miller")
+    L.append("// value is wanted; kOpMillerDone emits group D")
+    L.append("constexpr uint32_t kOpLoadCorr = %d, kOpMillerDone = %d, kOpLoadLines = %d, kCondMl = 0x%xu;"
+             % (OP_LOAD_CORR, OP_MILLER_DONE, OP_LOAD_LINES, COND_ML))
     L.append("constexpr int kTGroup = %d;" % T_GROUP)
-    L.append("constexpr int kSeqLen = %d;" % len(seq))
-    L.append("__device__ __constant__ uint32_t kSeq[%d] = {" % len(seq))
-    words = [encode_op(op) for op in seq]
-    for i in range(0, len(words), 8):
-        L.append("    " + ", ".join("0x%05xu" % w for w in words[i:i + 8]) + ",")
+    seqs = [driver_sequence(False), driver_sequence(True)]
+    n = max(len(q) for q in seqs)
+    L.append("constexpr int kSeqLenRaw = %d, kSeqLenNorm = %d;" % (len(seqs[0]), len(seqs[1])))
+    L.append("__device__ __constant__ uint32_t kSeq[2][%d] = {" % n)
+    for seq in seqs:
+        words = [encode_op(op) for op in seq] + [0] * (n - len(seq))
+        L.append("  {")
+        for i in range(0, len(words), 8):
+            L.append("    " + ", ".join("0x%05xu" % w for w in words[i:i + 8]) + ",")
+        L.append("  },")
     L.append("};")
     L.append("// QP[h] = floor(h * 2^381 / p) * p, 13 words padded to 16")
     L.append("__device__ const uint32_t kQP2[128][16] = {")

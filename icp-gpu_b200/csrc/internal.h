@@ -22,11 +22,22 @@ struct VerifyArgs {
     uint64_t* gt_out;            // n x 72 or NULL, device
     const uint64_t* sig_xy;      // decoded signatures (n x 12 u64) when sigs were compressed, device
     int* work_counter;           // persistent mode: items are claimed from this zeroed counter, device
+    // Normalised line tables (every row divided by its c2) and the Miller
+    // correction factors (Fp2, 12 u64) of the generator and the keys, device;
+    // pk_norm NULL = use the raw tables.  Read by the Fp2-lane kernel only.
+    const uint64_t* g2_norm;
+    const uint64_t* pk_norm;
+    const uint64_t* g2_corr;
+    const uint64_t* pk_corr;
 };
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
 cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStream_t s);
+// n line tables divided row by row by their c2, with each table's Miller
+// correction factor (12 u64) and a flag set when a c2 is zero (table copied)
+cudaError_t launch_lines_normalize(const uint64_t* raw, int n, uint64_t* norm, uint64_t* corr, uint8_t* bad,
+                                   cudaStream_t s);
 // lane-parallel verify; in_status: per-item decode status or NULL.  lanes 6
 // runs the Fp2-lane kernel (verify_fp2.cu), 2, 4 and 8 the interpreter of
 // per-Fp programs (verify_vm.cu).
@@ -47,6 +58,10 @@ struct CtxView {
     const uint64_t* pk_tables;
     const uint8_t* pk_identity;
     int n_pks;
+    const uint64_t* g2_norm;     // NULL: raw lines only
+    const uint64_t* pk_norm;
+    const uint64_t* g2_corr;
+    const uint64_t* pk_corr;
 };
 
 }  // namespace bls

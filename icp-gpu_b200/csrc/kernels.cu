@@ -67,6 +67,64 @@ __global__ void __launch_bounds__(64) k_g2_prepare(const uint64_t* q, int n, uin
     g2_prepare(qx, qy, out + BLS_COEFF_U64 * (size_t)i);
 }
 
+// One line table per thread: every row (c0, c1, c2) becomes (c0 / c2, c1 / c2, 1)
+// (inverses by Montgomery's batch trick: one Fp2 inverse per table), and the
+// Miller correction factor prod_i c2_i^(2^(squarings after line i)) follows the
+// Miller loop's order of lines and squarings (api.cu:30-52).  A table with a
+// zero c2 is copied unchanged and flagged.
+__global__ void __launch_bounds__(64) k_lines_normalize(const uint64_t* raw, int n, uint64_t* norm, uint64_t* corr,
+                                                      uint8_t* bad) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint64_t* in = raw + BLS_COEFF_U64 * (size_t)t;
+    uint64_t* out = norm + BLS_COEFF_U64 * (size_t)t;
+    constexpr int kRows = 68;
+    auto c2_of = [&](int i) { return fp2{fp_load_u64(in + 36 * i + 24), fp_load_u64(in + 36 * i + 30)}; };
+    // prefix products of c2 in the output's c2 slots
+    fp2 pre = fp2_one();
+    for (int i = 0; i < kRows; ++i) {
+        pre = fp2_mul(pre, c2_of(i));
+        store_fp2(out + 36 * i + 24, pre);
+    }
+    if (fp2_is_zero(pre)) {
+        for (int i = 0; i < BLS_COEFF_U64; ++i) out[i] = in[i];
+        store_fp2(corr + 12 * (size_t)t, fp2_one());
+        bad[t] = 1;
+        return;
+    }
+    fp2 inv = fp2_inv(pre);   // (c2_0 ... c2_67)^-1
+    for (int i = kRows - 1; i >= 0; --i) {
+        fp2 c2 = c2_of(i);
+        fp2 inv_i = i ? fp2_mul(inv, fp2{fp_load_u64(out + 36 * (i - 1) + 24), fp_load_u64(out + 36 * (i - 1) + 30)})
+                      : inv;
+        inv = fp2_mul(inv, c2);
+        fp2 c0 = {fp_load_u64(in + 36 * i), fp_load_u64(in + 36 * i + 6)};
+        fp2 c1 = {fp_load_u64(in + 36 * i + 12), fp_load_u64(in + 36 * i + 18)};
+        store_fp2(out + 36 * i, fp2_mul(c0, inv_i));
+        store_fp2(out + 36 * i + 12, fp2_mul(c1, inv_i));
+    }
+    for (int i = 0; i < kRows; ++i) store_fp2(out + 36 * i + 24, fp2_one());
+    // correction factor
+    const uint64_t xabs = 0xd201000000010000ULL;
+    fp2 cf = fp2_one();
+    int ci = 0;
+    for (int b = 61; b >= 0; --b) {
+        cf = fp2_mul(cf, c2_of(ci++));
+        if (((xabs >> 1) >> b) & 1) cf = fp2_mul(cf, c2_of(ci++));
+        cf = fp2_sqr(cf);
+    }
+    cf = fp2_mul(cf, c2_of(ci));
+    store_fp2(corr + 12 * (size_t)t, cf);
+    bad[t] = 0;
+}
+
+cudaError_t launch_lines_normalize(const uint64_t* raw, int n, uint64_t* norm, uint64_t* corr, uint8_t* bad,
+                                   cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_lines_normalize<<<(n + 63) / 64, 64, 0, s>>>(raw, n, norm, corr, bad);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s) {
     if (a.n <= 0) return cudaSuccess;
     if (a.sig_xy) return cudaErrorInvalidValue;

@@ -102,6 +102,10 @@ struct bls_server {
         a.nhms = (const uint64_t*)s.d_nhms;
         a.g2 = view.g2;
         a.pk_tables = view.pk_tables;
+        a.g2_norm = view.g2_norm;
+        a.pk_norm = view.pk_norm;
+        a.g2_corr = view.g2_corr;
+        a.pk_corr = view.pk_corr;
         a.pk_index = (const int32_t*)s.d_ids;
         a.pk_identity = view.pk_identity;
         a.n = (int)n;

@@ -95,9 +95,17 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
     }
     for (uint32_t t = 0; t < nt; ++t) {
         const uint32_t w = f2::kDesc[off + 2 + t];
-        const uint32_t kind = w & 3u, xi = (w >> 2) & 1u, neg = (w >> 3) & 1u, dbl = (w >> 4) & 1u,
-                       yim = (w >> 5) & 1u, mask = (w >> 24) & 7u;
+        const uint32_t kind = w & 7u, xi = (w >> 3) & 1u, neg = (w >> 4) & 1u, dbl = (w >> 5) & 1u,
+                       yim = (w >> 6) & 1u, mask = (w >> 24) & 7u;
         const uint32_t xs = slot_addr(bs, (w >> 8) & 0x7fu), ys = slot_addr(bs, (w >> 16) & 0x7fu);
+        if (kind == f2::kOne) {             // X R: X into the high half of both accumulators
+            uint32_t x0[12], x1[12];
+            load_fp(x0, sm, xs, 0);
+            load_fp(x1, sm, xs, 1);
+            f2::acc_add_hi(acc[0], x0, neg);
+            f2::acc_add_hi(acc[1], x1, neg);
+            continue;
+        }
         // operands of products 0 and 1: (A0, B0), (A1, B1); KARA's product 2 is (A0 + A1, B0 + B1)
         uint32_t A0[12], A1[12], B0[12], B1[12];
         load_fp(A0, sm, xs, 0);
@@ -347,6 +355,9 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
     c.lane = c.active ? lane32 % kLanes : 6 + (lane32 & 1);
     c.region = kKSlots + (c.active ? pi : 0) * kPairSlots;
     uint32_t* bcast = sm + kSlotArea + kXchArea + 2 * kPairsPerBlock;
+    // normalised line tables (every row divided by its c2) when the caller has them
+    const int norm = a.pk_norm != nullptr ? 1 : 0;
+    const uint64_t* g2_lines = norm ? a.g2_norm : a.g2;
 
     int next = blockIdx.x * kPairsPerBlock;
     const int stride = gridDim.x * kPairsPerBlock;
@@ -365,7 +376,8 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
         const int item = base + (c.active ? pi : 0);
         const bool have = c.active && item < a.n;
         bool skip1 = true, skip2 = true;
-        const uint64_t* pk = a.g2;
+        const uint64_t* pk = g2_lines;
+        const uint64_t* pk_cf = a.g2_corr;
         int32_t status = 0;
         if (have) {
             const uint64_t* s = a.sig_xy ? a.sig_xy + 12 * (size_t)item : (const uint64_t*)a.sigs + 12 * (size_t)item;
@@ -374,7 +386,8 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
             fp sx = fp_load_u64(s), sy = fp_load_u64(s + 6);
             fp hx = fp_load_u64(h), hy = fp_load_u64(h + 6);
             int64_t pki = a.pk_index ? (int64_t)a.pk_index[item] : (int64_t)item;
-            pk = a.pk_tables + kCoeffU64 * pki;
+            pk = (norm ? a.pk_norm : a.pk_tables) + kCoeffU64 * pki;
+            if (norm) pk_cf = a.pk_corr + 12 * pki;
             skip1 = g1_limbs_identity(sx, sy) || status != 0;
             skip2 = g1_limbs_identity(hx, hy) || (a.pk_identity && a.pk_identity[pki]) || status != 0;
             if (c.lane == 0 && c.half == 0) {
@@ -397,13 +410,25 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
 
         // the op sequence: Miller loop over |x| >> 1 below its leading bit
         // (api.cu:30-52), then the final exponentiation (api.cu:65-78)
-        for (int s = 0; s < f2::kSeqLen; ++s) {
-            const uint32_t e = f2::kSeq[s];
+        const int seq_len = norm ? f2::kSeqLenNorm : f2::kSeqLenRaw;
+        for (int s = 0; s < seq_len; ++s) {
+            const uint32_t e = f2::kSeq[norm][s];
             const uint32_t code = e & 31u;
+            if ((e & f2::kCondMl) && !a.ml_out) continue;
             if (code == f2::kOpLoadLines) {
-                load_lines(c, a.g2, skip1, pk, skip2, (int)(e >> 14));
+                load_lines(c, g2_lines, skip1, pk, skip2, (int)((e >> 14) & 127u));
+            } else if (code == f2::kOpLoadCorr) {
+                // the generator's and the key's Miller correction factors into the c2 slots
+                if (c.active && c.lane < 2) {
+                    const bool skip = c.lane ? skip2 : skip1;
+                    const uint64_t* cf = c.lane ? pk_cf : a.g2_corr;
+                    const uint32_t slot = c.region + kCOff + 6 * c.lane + 2;
+                    if (skip) store_fp(sm, slot, c.half, c.half ? fp_zero().w : fp_one().w);
+                    else copy_fp_from_global(sm, slot, c.half, cf + 6 * c.half);
+                }
+                __syncthreads();
             } else if (code == f2::kOpMillerDone) {
-                if (a.ml_out) emit_group(c, 0, have ? a.ml_out + 72 * (size_t)item : nullptr);
+                if (a.ml_out) emit_group(c, (e >> 5) & 7u, have ? a.ml_out + 72 * (size_t)item : nullptr);
             } else {
                 Bases bs;
                 bs.b[0] = grp(c, (e >> 5) & 7u);

@@ -11,6 +11,8 @@ import gen_fp2ops as G  # noqa: E402
 
 import bls_ref as B  # noqa: E402
 
+X_ABS = G.X_ABS
+
 
 K_SLOTS = 8
 GROUPS = 7
@@ -68,9 +70,43 @@ class Machine:
         return out
 
 
-def verify(sig, nhm, g2_limbs, pk_limbs, skip1=False, skip2=False):
+def table_f2(tab, ci, k):
+    w = [int(x) for x in tab[36 * ci + 12 * k: 36 * ci + 12 * k + 12]]
+    return (sum(x << (64 * i) for i, x in enumerate(w[:6])), sum(x << (64 * i) for i, x in enumerate(w[6:])))
+
+
+def normalise_table(tab):
+    """(coefficient rows (c0 / c2, c1 / c2, 1) in Montgomery form, Miller
+    correction factor): the line table divided row by row by its c2, and
+    prod_i c2_i^(2^(squarings after line i)), both as Montgomery Fp2."""
+    def dec(v):
+        return (v[0] * B.MONT_RINV % B.P, v[1] * B.MONT_RINV % B.P)
+
+    rows, corr = [], B.F2_ONE if hasattr(B, "F2_ONE") else (1, 0)
+    ci = 0
+
+    def line():
+        nonlocal ci, corr
+        c0, c1, c2 = (dec(table_f2(tab, ci, k)) for k in range(3))
+        inv = B.f2_inv(c2)
+        rows.append((f2m(B.f2_mul(c0, inv)), f2m(B.f2_mul(c1, inv)), (mont(1), 0)))
+        corr = B.f2_mul(corr, c2)
+        ci += 1
+
+    for b in range(61, -1, -1):
+        line()
+        if ((X_ABS >> 1) >> b) & 1:
+            line()
+        corr = B.f2_mul(corr, corr)
+    line()
+    return rows, f2m(corr)
+
+
+def verify(sig, nhm, g2_limbs, pk_limbs, skip1=False, skip2=False, normalised=False):
     """sig / nhm: canonical affine points; tables: 2448 u64.  Returns
-    (miller, gt) as canonical flat Fp lists (normal form)."""
+    (miller, gt) as canonical flat Fp lists (normal form).  `normalised` runs
+    the normalised-line sequence and multiplies the Miller value back by the
+    two correction factors, as the kernel does for registered keys."""
     m = Machine()
     C = m.region + C_OFF
     one = mont(1)
@@ -78,24 +114,30 @@ def verify(sig, nhm, g2_limbs, pk_limbs, skip1=False, skip2=False):
     for pair in range(2):
         m.slots[C + 6 * pair + G.C_PT] = (mont(pts[pair][0]), mont(pts[pair][1]))
     m.set_group(0, [(one, 0)] + [(0, 0)] * 5)
+    norm = [normalise_table(g2_limbs), normalise_table(pk_limbs)] if normalised else None
 
     def load(ci):
         for pair, (tab, skip) in enumerate(((g2_limbs, skip1), (pk_limbs, skip2))):
             for k in range(3):
                 if skip:
                     v = (one, 0) if k == 2 else (0, 0)
+                elif normalised:
+                    v = norm[pair][0][ci][k]
                 else:
-                    w = [int(x) for x in tab[36 * ci + 12 * k: 36 * ci + 12 * k + 12]]
-                    v = (sum(x << (64 * i) for i, x in enumerate(w[:6])), sum(x << (64 * i) for i, x in enumerate(w[6:])))
+                    v = table_f2(tab, ci, k)
                 m.slots[C + 6 * pair + k] = v
 
     names = [name for name, _, _ in G.PROGRAMS]
     ml = None
-    for code, d, a, b, ci in G.driver_sequence():
+    for code, d, a, b, ci in G.driver_sequence(normalised):
+        code &= ~G.COND_ML          # the Miller value is always wanted here
         if code == G.OP_LOAD_LINES:
             load(ci)
+        elif code == G.OP_LOAD_CORR:
+            for pair, skip in enumerate((skip1, skip2)):
+                m.slots[C + 6 * pair + G.C_C2] = (one, 0) if skip else norm[pair][1]
         elif code == G.OP_MILLER_DONE:
-            ml = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]
+            ml = [v * B.MONT_RINV % B.P for v in m.group_flat(d)]
         else:
             m.call(names[code], d, a, b)
     gt = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]

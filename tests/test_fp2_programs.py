@@ -92,14 +92,16 @@ def test_inverse_of_zero_is_zero():
     assert got(m, 2) == [0] * 12
 
 
-def test_full_verify_through_programs(golden):
+@pytest.mark.parametrize("normalised", [False, True], ids=["raw-lines", "normalised-lines"])
+def test_full_verify_through_programs(golden, normalised):
     sig = B.g1_from_mont_u64(golden["sig_294_g1"])
     nhm = B.g1_from_mont_u64(golden["neg_hm_7_g1"])
-    ml, gt = E.verify(sig, nhm, golden["g2_gen_coeffs"], golden["pk42_coeffs"])
+    ml, gt = E.verify(sig, nhm, golden["g2_gen_coeffs"], golden["pk42_coeffs"], normalised=normalised)
     assert B.f12_mont_limbs(B.f12_from_flat(ml))[:6] == list(golden["ml_2pair_c000"])
     assert B.f12_from_flat(gt) == B.F12_ONE
     # e(G1, G2) alone: the second pair skipped
-    ml, gt = E.verify(B.G1_GEN, None, golden["g2_gen_coeffs"], golden["pk42_coeffs"], skip2=True)
+    ml, gt = E.verify(B.G1_GEN, None, golden["g2_gen_coeffs"], golden["pk42_coeffs"], skip2=True,
+                      normalised=normalised)
     assert B.f12_mont_limbs(B.f12_from_flat(ml)) == list(golden["ml_g1_g2"])
     assert B.f12_mont_limbs(B.f12_from_flat(gt)) == list(golden["pairing_g1_g2"])
 
