@@ -306,8 +306,10 @@ def run_gpu(args):
     e2e_s = max_over_ranks(pg, sum(e2e_times), dev)
     e2e_value = whole_job_rate(N_ITEMS, world, args.steps, e2e_s)
 
-    batching = serving = None
+    batching = serving = ingest = None
     if not args.no_extras:
+        sizes = [int(v) for v in args.ingest_keys.split(",") if int(v) > 0]
+        ingest = [run_ingest(G, WL, local, args.lanes, k) for k in sizes] or None
         batching = run_batching(G, WL, ctx, ids)
         if args.serve_seconds > 0:
             serving = run_serving(G, WL, ctx, args.serve_seconds, slots=args.serve_slots,
@@ -346,6 +348,8 @@ def run_gpu(args):
             "gpu_launches": args.steps,
             "bit_exact": True,
         }
+        if ingest:
+            result["ingest"] = ingest
         if batching:
             result["batching"] = batching
         if serving:
@@ -382,6 +386,36 @@ def run_batching(G, WL, ctx, ids_unused, reps=2):
         out[name + "_ms"] = round(best * 1e3, 2)
     out["speedup"] = round(out["persistent_verifies_per_s"] / out["plain_verifies_per_s"], 2)
     return out
+
+
+def run_ingest(G, WL, device, lanes, n_keys, reps=3):
+    """Key ingest: n_keys 96-byte compressed public keys decoded, validated,
+    prepared and normalised on the GPU by one bls_pk_register_compressed call
+    (host-timed, best of reps, each on a fresh context), against the CPU line-table
+    precompute alone (the caller's per-key G2Prepared::from) on all host threads."""
+    rng = WL.SplitMix64(SEED + 17)
+    sks = np.array([WL.scalar_limbs(rng.scalar()) for _ in range(n_keys)], dtype=np.uint64)
+    q = WL.g2_mul_gen(sks)
+    enc = WL.g2_compress(q).tobytes()
+    best = 1e30
+    for _ in range(reps):
+        c = G.Context(device=device, lanes=lanes, max_pks=n_keys)
+        t0 = time.perf_counter()
+        ids, st = c.register_pk_compressed(enc)
+        best = min(best, time.perf_counter() - t0)
+        assert (st == 0).all()
+        check = [0, n_keys - 1]
+        want = WL.g2_prepare(q[check])
+        for j, i in enumerate(check):
+            assert (c.pk_table(int(ids[i])) == want[j]).all(), "ingested table differs"
+        c.close()
+    t0 = time.perf_counter()
+    WL.g2_prepare(q)
+    cpu_s = time.perf_counter() - t0
+    return {"keys": n_keys, "api": "bls_pk_register_compressed (decode + checks + tables + normalise)",
+            "gpu_keys_per_s": round(n_keys / best, 1), "gpu_ms": round(best * 1e3, 2),
+            "cpu_prepare_keys_per_s": round(n_keys / cpu_s, 1), "cpu_threads": WL.nthreads(),
+            "cpu_note": "CPU line-table precompute only (no decode or subgroup check)"}
 
 
 def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192):
@@ -470,6 +504,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batching and serving sections")
     ap.add_argument("--lanes", type=int, default=6, help="lanes per verification (6: Fp2-lane kernel; 1, 2, 4, 8)")
+    ap.add_argument("--ingest-keys", default="1024,16384",
+                    help="comma-separated key counts ingested compressed on the GPU (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the serving stream (0 = skip)")
     ap.add_argument("--serve-slots", type=int, default=3, help="serving: launches in flight")
     ap.add_argument("--serve-max-batch", type=int, default=8192, help="serving: items per launch")

@@ -37,7 +37,9 @@ SIG_AFFINE, SIG_COMPRESSED = 0, 1
 
 
 class GpuError(RuntimeError):
-    pass
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        self.status = status   # per-item decode status of a failed registration
 
 
 class Config(ctypes.Structure):
@@ -95,6 +97,8 @@ def lib():
         L.bls_last_error.restype = ctypes.c_char_p
         L.bls_pk_register_coeffs.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_int32)]
         L.bls_pk_register_affine.argtypes = [P, P, ctypes.POINTER(ctypes.c_int32)]
+        L.bls_pk_register_compressed.argtypes = [P, P, I, P, P]
+        L.bls_g2_decompress_status.argtypes = [P, P, I, P, P]
         L.bls_pk_table.argtypes = [P, ctypes.c_int32, P]
         L.bls_verify_batch.argtypes = [P, ctypes.POINTER(Batch), P]
         L.bls_verify_batch_device.argtypes = [P, ctypes.POINTER(Batch), P]
@@ -246,6 +250,30 @@ class Context:
         pid = ctypes.c_int32()
         self._check(self.lib.bls_pk_register_affine(self.h, _ptr(q), ctypes.byref(pid)), "bls_pk_register_affine")
         return pid.value
+
+    def register_pk_compressed(self, pks96):
+        """Decode, validate and prepare n 96-byte keys on the GPU.  Returns
+        (ids, status); raises GpuError (registering none) when a key fails."""
+        src = np.ascontiguousarray(np.frombuffer(bytes(pks96), dtype=np.uint8))
+        assert src.size % 96 == 0
+        n = src.size // 96
+        ids = np.full(n, -1, dtype=np.int32)
+        st = np.zeros(n, dtype=np.int32)
+        rc = self.lib.bls_pk_register_compressed(self.h, _ptr(src), n, _ptr(ids), _ptr(st))
+        if rc != BLS_OK:
+            raise GpuError("bls_pk_register_compressed failed (%d): %s" % (rc, last_error()), status=st)
+        return ids, st
+
+    def g2_decompress(self, compressed):
+        """(status (n,) int32, q (n, 24) u64: x.c0, x.c1, y.c0, y.c1 Montgomery)."""
+        src = np.ascontiguousarray(np.frombuffer(bytes(compressed), dtype=np.uint8))
+        assert src.size % 96 == 0
+        n = src.size // 96
+        q = np.zeros((n, 24), dtype=np.uint64)
+        st = np.zeros(n, dtype=np.int32)
+        self._check(self.lib.bls_g2_decompress_status(self.h, _ptr(src), n, _ptr(q), _ptr(st)),
+                    "bls_g2_decompress_status")
+        return st, q
 
     def pk_table(self, pk_id):
         out = np.zeros(G2_COEFF_U64S, dtype=np.uint64)

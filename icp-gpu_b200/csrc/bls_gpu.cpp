@@ -99,13 +99,15 @@ struct bls_ctx {
     uint8_t* d_norm_bad = nullptr;  // (1 + max_pks): a table with a zero c2
     bool norm_ok = true;            // every table normalised
 
-    // normalise table `src` into `dst`, correction factor into slot `k` of d_corr
-    int normalize(const uint64_t* src, uint64_t* dst, int k) {
+    // normalise table `src` into `dst`, correction factor into slot `k` of d_corr;
+    // an identity key's table is never read (its pair is skipped), so a zero
+    // c2 there does not disable the normalised path
+    int normalize(const uint64_t* src, uint64_t* dst, int k, bool identity = false) {
         CK(bls::launch_lines_normalize(src, 1, dst, d_corr + 12 * (size_t)k, d_norm_bad + k, stream));
         uint8_t bad = 0;
         CK(cudaMemcpyAsync(&bad, d_norm_bad + k, 1, cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
-        if (bad) norm_ok = false;
+        if (bad && !identity) norm_ok = false;
         return BLS_OK;
     }
     // normalised-line arguments of a verify over the registered tables
@@ -377,7 +379,7 @@ int bls_pk_register_coeffs(bls_ctx* ctx, const uint64_t* coeffs, int is_identity
     ctx->h_pk_inf[id] = inf;
     CK(cudaMemcpyAsync(ctx->d_pk_inf + id, &ctx->h_pk_inf[id], 1, cudaMemcpyHostToDevice, ctx->stream));
     int nrc = ctx->normalize(ctx->d_pk + (size_t)id * bls::kCoeffU64, ctx->d_pk_norm + (size_t)id * bls::kCoeffU64,
-                             1 + id);
+                             1 + id, inf != 0);
     if (nrc) return nrc;
     ctx->n_pks++;
     *pk_id = id;
@@ -402,6 +404,68 @@ int bls_pk_register_affine(bls_ctx* ctx, const uint64_t* q24, int32_t* pk_id) {
     if (nrc) return nrc;
     ctx->n_pks++;
     *pk_id = id;
+    return BLS_OK;
+}
+
+// Keys n_pks .. n_pks + n - 1 are decoded, prepared and normalised on the
+// device in one launch each; nothing is registered unless every key decodes.
+int bls_pk_register_compressed(bls_ctx* ctx, const uint8_t* pks96, int n, int32_t* pk_ids, int32_t* status) {
+    if (!ctx || (n > 0 && (!pks96 || !pk_ids))) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (n == 0) return BLS_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n > ctx->cfg.max_pks - ctx->n_pks)
+        return fail(BLS_ERR_FULL, "%d keys do not fit: %d of %d pk slots used", n, ctx->n_pks, ctx->cfg.max_pks);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int rc;
+    const size_t k = (size_t)n;
+    if ((rc = ctx->grow(ctx->d_in, k * 96)) || (rc = ctx->grow(ctx->d_xy, k * 192)) ||
+        (rc = ctx->grow(ctx->d_st, k * 4)))
+        return rc;
+    const int id0 = ctx->n_pks;
+    uint64_t* tables = ctx->d_pk + (size_t)id0 * bls::kCoeffU64;
+    std::vector<int32_t> st(k);
+    std::vector<uint8_t> inf(k), bad(k);
+    CK(cudaMemcpyAsync(ctx->d_in.p, pks96, k * 96, cudaMemcpyHostToDevice, ctx->stream));
+    CK(bls::launch_g2_decompress((const uint8_t*)ctx->d_in.p, n, (uint64_t*)ctx->d_xy.p, (int32_t*)ctx->d_st.p,
+                                 ctx->d_pk_inf + id0, ctx->stream));
+    CK(cudaMemcpyAsync(st.data(), ctx->d_st.p, k * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (status) memcpy(status, st.data(), k * 4);
+    for (size_t i = 0; i < k; ++i)
+        if (st[i] != BLS_ST_OK) return fail(BLS_ERR_INVALID, "key %zu: decode status %d", i, st[i]);
+    CK(bls::launch_g2_prepare((const uint64_t*)ctx->d_xy.p, n, tables, ctx->stream));
+    CK(bls::launch_lines_normalize(tables, n, ctx->d_pk_norm + (size_t)id0 * bls::kCoeffU64,
+                                   ctx->d_corr + 12 * (size_t)(1 + id0), ctx->d_norm_bad + 1 + id0, ctx->stream));
+    CK(cudaMemcpyAsync(inf.data(), ctx->d_pk_inf + id0, k, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(bad.data(), ctx->d_norm_bad + 1 + id0, k, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < k; ++i) {
+        ctx->h_pk_inf[id0 + i] = inf[i];
+        if (bad[i] && !inf[i]) ctx->norm_ok = false;
+        pk_ids[i] = id0 + (int32_t)i;
+    }
+    ctx->n_pks += n;
+    return BLS_OK;
+}
+
+int bls_g2_decompress_status(bls_ctx* ctx, const uint8_t* in, int n, uint64_t* q24, int32_t* status) {
+    if (!ctx || (n > 0 && (!in || !q24 || !status))) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (n == 0) return BLS_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int rc;
+    const size_t k = (size_t)n;
+    if ((rc = ctx->grow(ctx->d_in, k * 96)) || (rc = ctx->grow(ctx->d_xy, k * 192)) ||
+        (rc = ctx->grow(ctx->d_st, k * 4)))
+        return rc;
+    CK(cudaMemcpyAsync(ctx->d_in.p, in, k * 96, cudaMemcpyHostToDevice, ctx->stream));
+    CK(bls::launch_g2_decompress((const uint8_t*)ctx->d_in.p, n, (uint64_t*)ctx->d_xy.p, (int32_t*)ctx->d_st.p,
+                                 nullptr, ctx->stream));
+    CK(cudaMemcpyAsync(q24, ctx->d_xy.p, k * 192, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(status, ctx->d_st.p, k * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return BLS_OK;
 }
 

@@ -33,6 +33,8 @@ struct VerifyArgs {
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
+cudaError_t launch_g2_decompress(const uint8_t* in, int n, uint64_t* q, int32_t* status, uint8_t* identity,
+                                 cudaStream_t s);
 cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStream_t s);
 // n line tables divided row by row by their c2, with each table's Miller
 // correction factor (12 u64) and a flag set when a c2 is zero (table copied)

@@ -7,10 +7,14 @@
 //                     address (broadcast); public-key tables are read per item.
 //   k_g1_decompress   one 48-byte point per thread (cuda/decompress.cu:140-188)
 //                     plus the from_compressed checks.
+//   k_g2_decompress   one 96-byte compressed public key per thread, with the
+//                     G2Affine::from_compressed checks (no reference kernel: the
+//                     reference's callers decode keys on the CPU).
 //   k_g2_prepare      one G2 line table per thread (cuda/test_miller_v2.cu:148-229).
 #include <cuda_runtime.h>
 
 #include "g1.cuh"
+#include "g2.cuh"
 #include "g2prep.cuh"
 #include "internal.h"
 
@@ -56,6 +60,22 @@ __global__ void __launch_bounds__(128) k_g1_decompress(const uint8_t* in, int n,
     status[i] = st;
     fp_store_u64(xy + 12 * (size_t)i, x);
     fp_store_u64(xy + 12 * (size_t)i + 6, y);
+}
+
+// q: 24 x uint64 per key (x.c0, x.c1, y.c0, y.c1 Montgomery; zeros for the
+// identity and for a failure); identity (optional): 1 for the identity.
+__global__ void __launch_bounds__(64) k_g2_decompress(const uint8_t* in, int n, uint64_t* q, int32_t* status,
+                                                      uint8_t* identity) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    fp2 x, y;
+    bool id;
+    int32_t st = g2_decode(in + 96 * (size_t)i, x, y, id);
+    status[i] = st;
+    uint64_t* qi = q + 24 * (size_t)i;
+    store_fp2(qi, x);
+    store_fp2(qi + 12, y);
+    if (identity) identity[i] = (st == ST_OK && id) ? 1 : 0;
 }
 
 __global__ void __launch_bounds__(64) k_g2_prepare(const uint64_t* q, int n, uint64_t* out) {
@@ -136,6 +156,13 @@ cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s) {
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     k_g1_decompress<<<(n + 127) / 128, 128, 0, s>>>(in, n, xy, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g2_decompress(const uint8_t* in, int n, uint64_t* q, int32_t* status, uint8_t* identity,
+                                 cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_g2_decompress<<<(n + 63) / 64, 64, 0, s>>>(in, n, q, status, identity);
     return cudaGetLastError();
 }
 

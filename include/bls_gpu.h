@@ -20,6 +20,8 @@
  *           c0.c0.c0, c0.c0.c1, c0.c1.c0, ..., c1.c2.c1.
  *   Compressed G1  48 bytes, ZCash BLS12-381 encoding (big-endian x, flags
  *           0x80 compressed, 0x40 infinity, 0x20 y lexicographically largest).
+ *   Compressed G2  96 bytes, the same encoding of x = x.c1 || x.c0 (flags in
+ *           the top bits of x.c1's first byte).
  *
  * All pointers are host memory owned by the caller unless a name says
  * "device".  Every entry point is thread-safe.
@@ -96,7 +98,7 @@ int gpu_jacobian_to_affine(const uint8_t* jacobian, uint8_t* affine);
 #define BLS_ST_OK 0
 #define BLS_ST_BAD_FLAGS 1         /* compression bit clear, or infinity with payload / sort bit */
 #define BLS_ST_X_NOT_CANONICAL 2   /* x >= p */
-#define BLS_ST_NOT_ON_CURVE 3      /* x^3 + 4 is not a square */
+#define BLS_ST_NOT_ON_CURVE 3      /* x^3 + 4 (G2: x^3 + 4(1 + u)) is not a square */
 #define BLS_ST_NOT_IN_SUBGROUP 4   /* on the curve, outside the order-r subgroup */
 
 /* signature input formats */
@@ -144,6 +146,20 @@ int bls_pk_register_coeffs(bls_ctx* ctx, const uint64_t* coeffs2448, int is_iden
 /* From an affine point (x.c0, x.c1, y.c0, y.c1: 24 x uint64 Montgomery); the
  * line table is computed on the GPU.  The caller vouches that the point is in G2. */
 int bls_pk_register_affine(bls_ctx* ctx, const uint64_t* q24, int32_t* pk_id);
+/* From n 96-byte compressed keys (ZCash encoding: x.c1 || x.c0 big-endian,
+ * flags in byte 0 as for G1; x^3 + 4(1 + u) must be a square in Fp2 and the
+ * point in G2).  Decoding, every G2Affine::from_compressed check, the line
+ * tables and their normalisation all run on the GPU; this replaces the
+ * per-item CPU G2Prepared::from of the reference's callers
+ * (ic-integration/patches/ic-gpu-consensus.patch:458-461).  pk_ids[i] gets
+ * key i's id; status (optional, n entries) gets each key's BLS_ST_* code.
+ * All or nothing: when any key fails to decode, none is registered and the
+ * call returns BLS_ERR_INVALID.  The identity encoding (0xc0, zeros)
+ * registers an identity key, as bls_pk_register_coeffs with is_identity. */
+int bls_pk_register_compressed(bls_ctx* ctx, const uint8_t* pks96, int n, int32_t* pk_ids, int32_t* status);
+/* Decode n compressed G2 points: status[i] (BLS_ST_*), q24[i] 24 x uint64
+ * x.c0, x.c1, y.c0, y.c1 Montgomery (identity and failures: zeros). */
+int bls_g2_decompress_status(bls_ctx* ctx, const uint8_t* compressed96, int n, uint64_t* q24, int32_t* status);
 /* copy a registered table back (tests) */
 int bls_pk_table(bls_ctx* ctx, int32_t pk_id, uint64_t* coeffs2448);
 
