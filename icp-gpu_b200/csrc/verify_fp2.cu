@@ -79,6 +79,19 @@ __device__ __forceinline__ void store_fp(uint32_t* sm, uint32_t slot, int comp, 
 
 __device__ __forceinline__ int sext4(uint32_t v) { return (int)(v << 28) >> 28; }
 
+// P into the two accumulators with coefficients ca, cb (bit 0 nonzero, bit 1 negative)
+__device__ __forceinline__ void acc_pair(uint32_t* acc0, uint32_t* acc1, const uint32_t* P, uint32_t ca,
+                                         uint32_t cb) {
+    if (ca & 1u) {
+        if (ca >> 1) f2::acc_sub(acc0, P);
+        else f2::acc_plus(acc0, P);
+    }
+    if (cb & 1u) {
+        if (cb >> 1) f2::acc_sub(acc1, P);
+        else f2::acc_plus(acc1, P);
+    }
+}
+
 // Phase 1 of an output (product modes): this half's products into both
 // accumulators, acc[1 - half] left in the exchange slot for the partner.
 __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bases& bs, uint32_t* xch_out,
@@ -147,34 +160,24 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
                 B1[i] = A1[i];
             }
         }
-        // coefficients in {-1, 0, 1}: bit 0 nonzero, bit 1 negative (4 bits per product)
+        // coefficients in {-1, 0, 1}: bit 0 nonzero, bit 1 negative (4 bits per product).
+        // Products (A0, B0), (A1, B1), then KARA's (A0 + A1, B0 + B1) with the sums
+        // formed in place: no operand copies stay live beside the accumulators.
         const uint32_t cw = f2::kCoef[2 * kind + xi] ^ (neg ? 0x666666u : 0u);
-        const uint32_t np = kind == f2::kKara ? 3u : 2u;
-#pragma unroll 1
-        for (uint32_t j = 0; j < np; ++j) {
-            if (!((mask >> j) & 1u)) continue;
-            uint32_t U[12], V[12];
-            if (j == 2) {
-                f2::add12(U, A0, A1);
-                f2::add12(V, B0, B1);
-            } else {
-#pragma unroll
-                for (int i = 0; i < 12; ++i) {
-                    U[i] = j ? A1[i] : A0[i];
-                    V[i] = j ? B1[i] : B0[i];
-                }
-            }
-            uint32_t P[24];
-            f2::prod24(P, U, V);
-            const uint32_t ca = (cw >> (4 * j)) & 3u, cb = (cw >> (4 * (3 + j))) & 3u;
-            if (ca & 1u) {
-                if (ca >> 1) f2::acc_sub(acc[0], P);
-                else f2::acc_plus(acc[0], P);
-            }
-            if (cb & 1u) {
-                if (cb >> 1) f2::acc_sub(acc[1], P);
-                else f2::acc_plus(acc[1], P);
-            }
+        uint32_t P[24];
+        if (mask & 1u) {
+            f2::prod24(P, A0, B0);
+            acc_pair(acc[0], acc[1], P, cw & 3u, (cw >> 12) & 3u);
+        }
+        if (mask & 2u) {
+            f2::prod24(P, A1, B1);
+            acc_pair(acc[0], acc[1], P, (cw >> 4) & 3u, (cw >> 16) & 3u);
+        }
+        if (kind == f2::kKara && (mask & 4u)) {
+            f2::add12(A0, A0, A1);
+            f2::add12(B0, B0, B1);
+            f2::prod24(P, A0, B0);
+            acc_pair(acc[0], acc[1], P, (cw >> 8) & 3u, (cw >> 20) & 3u);
         }
     }
     uint4* x = reinterpret_cast<uint4*>(xch_out);
