@@ -478,7 +478,7 @@ PROGRAMS = [
 X_ABS = 0xd201000000010000
 OP_LOAD_CORR, OP_MILLER_DONE, OP_LOAD_LINES = 29, 30, 31
 COND_ML = 1 << 21     # op runs only when the Miller value is wanted
-T_GROUP = 3       # the inverse's temporaries use groups 3-5 from slot 0
+T_GROUP = 3       # the inverse's temporaries start at group 3's slot 0
 
 
 def driver_sequence(normalised=False):
@@ -520,33 +520,62 @@ def driver_sequence(normalised=False):
         for k in range(1, 9):
             prog("INV%d" % k, d, a)
 
-    def cyc_exp(dst, x, spare):
+    def cyc_exp(dst, x):
+        # programs may overwrite their inputs, so the products run in place
         prog("COPY", dst, x)
-        cur, oth = dst, spare
         for i in range(62, -1, -1):
-            prog("CYCSQR", cur, cur)
+            prog("CYCSQR", dst, dst)
             if (X_ABS >> i) & 1:
-                prog("MUL", oth, cur, x)
-                cur, oth = oth, cur
-        prog("CONJ", dst, cur)
+                prog("MUL", dst, dst, x)
+        prog("CONJ", dst, dst)
 
     # final exponentiation of group 0 into group 0: the reference's chain,
-    # api.cu:65-78, over seven groups
+    # api.cu:65-78, over six groups
     prog("CONJ", 1, 0); inv(2, 0); prog("MUL", 3, 1, 2); prog("FROB", 0, 3); prog("FROB", 1, 0)
     prog("MUL", 2, 1, 3); prog("COPY", 0, 2); prog("CYCSQR", 0, 0); prog("CONJ", 0, 0)
-    cyc_exp(1, 2, 3)
+    cyc_exp(1, 2)
     prog("MUL", 3, 0, 1)
-    cyc_exp(0, 3, 4)
+    cyc_exp(0, 3)
     prog("CONJ", 3, 3); prog("MUL", 4, 2, 3); prog("COPY", 3, 1); prog("CYCSQR", 3, 3)
-    cyc_exp(5, 0, 6)
-    prog("MUL", 6, 1, 5); prog("FROB", 1, 6); prog("FROB", 6, 1); prog("MUL", 1, 4, 6)
-    cyc_exp(4, 5, 6)
+    cyc_exp(5, 0)
+    prog("MUL", 1, 1, 5); prog("FROB", 1, 1); prog("FROB", 1, 1); prog("MUL", 1, 4, 1)
+    cyc_exp(4, 5)
     prog("MUL", 5, 3, 4)
-    cyc_exp(3, 5, 4)
+    cyc_exp(3, 5)
     prog("MUL", 4, 1, 3); prog("CONJ", 1, 2); prog("MUL", 3, 5, 1); prog("MUL", 1, 2, 0)
     prog("FROB", 0, 1); prog("FROB", 2, 0); prog("FROB", 0, 2); prog("MUL", 1, 4, 0); prog("FROB", 2, 3)
     prog("MUL", 0, 1, 2)
     return seq
+
+
+def t_slots_used():
+    """Temporary slots (base T) any program reads or writes."""
+    hi = -1
+    for name, fn, _ in PROGRAMS:
+        for o in fn():
+            if o is None:
+                continue
+            refs = [o.dst] + [r for t in o.terms for r in (t.x, t.y) if r is not None] + \
+                   [l[1] for l in o.lins]
+            hi = max([hi] + [r & 15 for r in refs if isinstance(r, int) and (r >> 4) == B_T])
+    return hi + 1
+
+
+def groups_used(seqs):
+    """Groups of six Fp2 slots the op sequences need per verification."""
+    n_prog = len(PROGRAMS)
+    t_slots = t_slots_used()
+    hi = 0
+    for seq in seqs:
+        for code, d, a, b, _ in seq:
+            code &= ~COND_ML
+            if code < n_prog:
+                hi = max(hi, d, a, b)
+                if PROGRAMS[code][0].startswith("INV"):
+                    hi = max(hi, T_GROUP + (t_slots - 1) // 6)
+            elif code == OP_MILLER_DONE:
+                hi = max(hi, d)
+    return hi + 1
 
 
 def encode_op(op):
@@ -789,6 +818,8 @@ def emit(path):
              % (OP_LOAD_CORR, OP_MILLER_DONE, OP_LOAD_LINES, COND_ML))
     L.append("constexpr int kTGroup = %d;" % T_GROUP)
     seqs = [driver_sequence(False), driver_sequence(True)]
+    L.append("// Fp12 groups the sequences touch (operands, results, the inverse's temporaries)")
+    L.append("constexpr int kGroupsUsed = %d;" % groups_used(seqs))
     n = max(len(q) for q in seqs)
     L.append("constexpr int kSeqLenRaw = %d, kSeqLenNorm = %d;" % (len(seqs[0]), len(seqs[1])))
     L.append("__device__ __constant__ uint32_t kSeq[2][%d] = {" % n)

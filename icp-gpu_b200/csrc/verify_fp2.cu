@@ -36,7 +36,7 @@ namespace {
 constexpr int kLanes = 6;
 constexpr int kPairsPerBlock = 5;
 constexpr int kThreads = 64;                    // two halves of 32
-constexpr int kGroups = 7;
+constexpr int kGroups = f2::kGroupsUsed;
 constexpr int kCOff = 6 * kGroups;              // C area after the groups
 constexpr int kPairSlots = kCOff + 12;          // Fp2 slots per pairing
 constexpr int kKSlots = f2::kKSlotCount;        // block-shared constants
@@ -55,12 +55,16 @@ struct Ctx {
     bool active;       // thread belongs to a pairing
 };
 
-struct Bases { uint32_t b[6]; };  // D, A, B, C, K, T: absolute slot of index 0
+// D, A, B, C, K, T: absolute slot of index 0, one byte each (every slot index
+// of a block is below 256), so a reference resolves with a shift, not an
+// indexed array
+struct Bases { uint64_t b; };
+static_assert(kKSlots + kPairsPerBlock * kPairSlots <= 256, "slot indices must fit a byte");
 
 __device__ __forceinline__ uint32_t grp(const Ctx& c, int g) { return c.region + 6 * g; }
 
 __device__ __forceinline__ uint32_t slot_addr(const Bases& bs, uint32_t ref) {
-    return bs.b[ref >> 4] + (ref & 15u);
+    return (uint32_t)(bs.b >> (8u * (ref >> 4))) % 256u + (ref & 15u);
 }
 
 __device__ __forceinline__ void load_fp(uint32_t* x, const uint32_t* sm, uint32_t slot, int comp) {
@@ -98,14 +102,15 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
                                            int half, uint32_t* own) {
     const uint32_t hdr = f2::kDesc[off], bias = f2::kDesc[off + 1];
     const uint32_t nt = (hdr >> 2) & 15u;
-    uint32_t acc[2][26];
+    // accO: component `half` (reduced by this thread), accX: the other one (sent
+    // to the partner); coefficients and biases are swapped for half 1
+    uint32_t accO[26], accX[26];
+    const uint32_t sw = half ? 8u : 0u, c0 = half ? 12u : 0u, c1 = half ? 0u : 12u;
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-#pragma unroll
-        for (int i = 0; i < 12; ++i) acc[c][i] = 0;
-        acc[c][25] = 0;
-        f2::set_kp(acc[c] + 12, (bias >> (8 * c)) & 0xffu);
-    }
+    for (int i = 0; i < 12; ++i) accO[i] = accX[i] = 0;
+    accO[25] = accX[25] = 0;
+    f2::set_kp(accO + 12, (bias >> sw) & 0xffu);
+    f2::set_kp(accX + 12, (bias >> (8u - sw)) & 0xffu);
     for (uint32_t t = 0; t < nt; ++t) {
         const uint32_t w = f2::kDesc[off + 2 + t];
         const uint32_t kind = w & 7u, xi = (w >> 3) & 1u, neg = (w >> 4) & 1u, dbl = (w >> 5) & 1u,
@@ -113,10 +118,10 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
         const uint32_t xs = slot_addr(bs, (w >> 8) & 0x7fu), ys = slot_addr(bs, (w >> 16) & 0x7fu);
         if (kind == f2::kOne) {             // X R: X into the high half of both accumulators
             uint32_t x0[12], x1[12];
-            load_fp(x0, sm, xs, 0);
-            load_fp(x1, sm, xs, 1);
-            f2::acc_add_hi(acc[0], x0, neg);
-            f2::acc_add_hi(acc[1], x1, neg);
+            load_fp(x0, sm, xs, half);
+            load_fp(x1, sm, xs, 1 - half);
+            f2::acc_add_hi(accO, x0, neg);
+            f2::acc_add_hi(accX, x1, neg);
             continue;
         }
         // operands of products 0 and 1: (A0, B0), (A1, B1); KARA's product 2 is (A0 + A1, B0 + B1)
@@ -167,28 +172,26 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
         uint32_t P[24];
         if (mask & 1u) {
             f2::prod24(P, A0, B0);
-            acc_pair(acc[0], acc[1], P, cw & 3u, (cw >> 12) & 3u);
+            acc_pair(accO, accX, P, (cw >> c0) & 3u, (cw >> c1) & 3u);
         }
         if (mask & 2u) {
             f2::prod24(P, A1, B1);
-            acc_pair(acc[0], acc[1], P, (cw >> 4) & 3u, (cw >> 16) & 3u);
+            acc_pair(accO, accX, P, (cw >> (c0 + 4)) & 3u, (cw >> (c1 + 4)) & 3u);
         }
         if (kind == f2::kKara && (mask & 4u)) {
             f2::add12(A0, A0, A1);
             f2::add12(B0, B0, B1);
             f2::prod24(P, A0, B0);
-            acc_pair(acc[0], acc[1], P, (cw >> 8) & 3u, (cw >> 20) & 3u);
+            acc_pair(accO, accX, P, (cw >> (c0 + 8)) & 3u, (cw >> (c1 + 8)) & 3u);
         }
     }
     uint4* x = reinterpret_cast<uint4*>(xch_out);
 #pragma unroll
-    for (int i = 0; i < 24; i += 4)
-        x[i / 4] = half ? make_uint4(acc[0][i], acc[0][i + 1], acc[0][i + 2], acc[0][i + 3])
-                        : make_uint4(acc[1][i], acc[1][i + 1], acc[1][i + 2], acc[1][i + 3]);
-    xch_out[24] = half ? acc[0][24] : acc[1][24];
-    xch_out[25] = half ? acc[0][25] : acc[1][25];
+    for (int i = 0; i < 24; i += 4) x[i / 4] = make_uint4(accX[i], accX[i + 1], accX[i + 2], accX[i + 3]);
+    xch_out[24] = accX[24];
+    xch_out[25] = accX[25];
 #pragma unroll
-    for (int i = 0; i < 26; ++i) own[i] = half ? acc[1][i] : acc[0][i];
+    for (int i = 0; i < 26; ++i) own[i] = accO[i];
 }
 
 // Phase 2: component `half` of the output into o (12 words).  own: this
@@ -434,12 +437,9 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
                 if (a.ml_out) emit_group(c, (e >> 5) & 7u, have ? a.ml_out + 72 * (size_t)item : nullptr);
             } else {
                 Bases bs;
-                bs.b[0] = grp(c, (e >> 5) & 7u);
-                bs.b[1] = grp(c, (e >> 8) & 7u);
-                bs.b[2] = grp(c, (e >> 11) & 7u);
-                bs.b[3] = c.region + kCOff;
-                bs.b[4] = 0;
-                bs.b[5] = grp(c, f2::kTGroup);
+                bs.b = (uint64_t)grp(c, (e >> 5) & 7u) | (uint64_t)grp(c, (e >> 8) & 7u) << 8 |
+                       (uint64_t)grp(c, (e >> 11) & 7u) << 16 | (uint64_t)(c.region + kCOff) << 24 |
+                       (uint64_t)grp(c, f2::kTGroup) << 40;
                 run((int)code, sm, c.pair, c.lane, c.half, bs);
             }
         }
