@@ -106,6 +106,8 @@ def lib():
         L.bls_ctx_stream.argtypes = [P]
         L.bls_ctx_stream.restype = P
         L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
+        L.bls_neg_hash_to_g1.argtypes = [P, P, P, I, P, I, P]
+        L.bls_verify_messages.argtypes = [P, I, P, P, P, P, I, P, I, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
         L.bls_verify_compressed_noalloc.argtypes = [P, P, P, P, P, P, I, I, P]
         L.bls_server_create.argtypes = [P, ctypes.POINTER(ServerConfig), ctypes.POINTER(P)]
@@ -118,6 +120,14 @@ def lib():
         L.bls_autotune.argtypes = [P, ctypes.POINTER(Batch), I, ctypes.POINTER(TunePoint), I, ctypes.POINTER(I)]
         _lib = L
     return _lib
+
+
+def pack_messages(msgs):
+    """Messages back to back (uint8) and their n + 1 byte offsets (uint32)."""
+    off = np.zeros(len(msgs) + 1, dtype=np.uint32)
+    off[1:] = np.cumsum([len(m) for m in msgs], dtype=np.uint64).astype(np.uint32)
+    buf = np.frombuffer(b"".join(bytes(m) for m in msgs) or b"\0", dtype=np.uint8).copy()
+    return buf, off
 
 
 def last_error():
@@ -311,6 +321,35 @@ class Context:
 
     def stream(self):
         return self.lib.bls_ctx_stream(self.h)
+
+    def neg_hash_to_g1(self, msgs, dst):
+        """-H(m) for each message (RFC 9380 hash_to_curve, SVDW suite) on the GPU: (n, 12) u64."""
+        buf, off = pack_messages(msgs)
+        d = np.frombuffer(bytes(dst), dtype=np.uint8).copy()
+        out = np.zeros((len(msgs), 12), dtype=np.uint64)
+        self._check(self.lib.bls_neg_hash_to_g1(self.h, _ptr(buf), _ptr(off), len(msgs), _ptr(d) if d.size else None,
+                                                d.size, _ptr(out)), "bls_neg_hash_to_g1")
+        return out
+
+    def verify_messages(self, sigs, msgs, pk_ids, dst, compressed=False):
+        """results (n,) int32 as verify(), with -H(m_i) computed on the GPU from the message bytes."""
+        n = len(msgs)
+        if compressed:
+            s = np.ascontiguousarray(np.frombuffer(bytes(sigs), dtype=np.uint8) if not isinstance(sigs, np.ndarray)
+                                     else sigs, dtype=np.uint8).reshape(-1)
+            assert s.size == 48 * n
+        else:
+            s = _u64(sigs, 12)
+            assert s.shape[0] == n
+        buf, off = pack_messages(msgs)
+        d = np.frombuffer(bytes(dst), dtype=np.uint8).copy()
+        ids = np.ascontiguousarray(pk_ids, dtype=np.int32).reshape(-1)
+        assert ids.size == n
+        res = np.zeros(n, dtype=np.int32)
+        self._check(self.lib.bls_verify_messages(self.h, SIG_COMPRESSED if compressed else SIG_AFFINE, _ptr(s),
+                                                 _ptr(buf), _ptr(off), _ptr(ids), n, _ptr(d) if d.size else None,
+                                                 d.size, _ptr(res)), "bls_verify_messages")
+        return res
 
     def g1_decompress(self, compressed):
         src = np.ascontiguousarray(np.frombuffer(bytes(compressed), dtype=np.uint8))

@@ -78,6 +78,7 @@ struct bls_ctx {
     };
     // per-call scratch
     DevBuf d_sigs, d_nhms, d_pkidx, d_res, d_ml, d_gt, d_pk_items, d_g2_call, d_in, d_xy, d_st, d_work;
+    DevBuf d_msg, d_off, d_dst;  // message bytes, offsets and domain of a hash
     HostBuf h_sigs, h_nhms, h_pkidx, h_res;
 
     // persistent batched launch captured as a CUDA graph, valid while the
@@ -156,7 +157,7 @@ struct bls_ctx {
     void release() {
         drop_graph();
         for (DevBuf* b : {&d_sigs, &d_nhms, &d_pkidx, &d_res, &d_ml, &d_gt, &d_pk_items, &d_g2_call, &d_in,
-                          &d_xy, &d_st, &d_work})
+                          &d_xy, &d_st, &d_work, &d_msg, &d_off, &d_dst})
             if (b->p) cudaFree(b->p);
         for (HostBuf* b : {&h_sigs, &h_nhms, &h_pkidx, &h_res})
             if (b->p) cudaFreeHost(b->p);
@@ -276,11 +277,14 @@ int prepare(bls_ctx* c, size_t n, int fmt, bool want_ml, bool want_gt) {
     return BLS_OK;
 }
 
-// enqueue: staged inputs -> device, verify, results -> h_res (no synchronise)
-int enqueue(bls_ctx* c, size_t n, int fmt, bool persistent, bool want_ml, bool want_gt) {
+// enqueue: staged inputs -> device, verify, results -> h_res (no synchronise);
+// nhms_on_device: d_nhms was filled on the device (a hash launch) instead
+int enqueue(bls_ctx* c, size_t n, int fmt, bool persistent, bool want_ml, bool want_gt,
+            bool nhms_on_device = false) {
     size_t sig_bytes = n * (fmt == BLS_SIG_COMPRESSED ? 48 : 96);
     CK(cudaMemcpyAsync(c->d_sigs.p, c->h_sigs.p, sig_bytes, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->d_nhms.p, c->h_nhms.p, n * 96, cudaMemcpyHostToDevice, c->stream));
+    if (!nhms_on_device)
+        CK(cudaMemcpyAsync(c->d_nhms.p, c->h_nhms.p, n * 96, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_pkidx.p, c->h_pkidx.p, n * 4, cudaMemcpyHostToDevice, c->stream));
     bls::VerifyArgs a{};
     a.sigs = c->d_sigs.p;
@@ -299,6 +303,32 @@ int enqueue(bls_ctx* c, size_t n, int fmt, bool persistent, bool want_ml, bool w
     int rc = run_verify(c, a);
     if (rc) return rc;
     CK(cudaMemcpyAsync(c->h_res.p, a.results, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    return BLS_OK;
+}
+
+// messages + offsets + domain to the device, then -H(m_i) into d_nhms
+int stage_hash(bls_ctx* c, const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst, int dst_len) {
+    if (offsets[0] != 0) return fail(BLS_ERR_INVALID, "offsets[0] must be 0");
+    for (int i = 0; i < n; ++i)
+        if (offsets[i + 1] < offsets[i]) return fail(BLS_ERR_INVALID, "offsets decrease at %d", i);
+    const size_t bytes = offsets[n];
+    int rc;
+    if ((rc = c->grow(c->d_msg, bytes ? bytes : 1)) || (rc = c->grow(c->d_off, ((size_t)n + 1) * 4)) ||
+        (rc = c->grow(c->d_dst, dst_len ? (size_t)dst_len : 1)) || (rc = c->grow(c->d_nhms, (size_t)n * 96)))
+        return rc;
+    if (bytes) CK(cudaMemcpyAsync(c->d_msg.p, msgs, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_off.p, offsets, ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, c->stream));
+    if (dst_len) CK(cudaMemcpyAsync(c->d_dst.p, dst, dst_len, cudaMemcpyHostToDevice, c->stream));
+    CK(bls::launch_neg_hash_to_g1((const uint8_t*)c->d_msg.p, (const uint32_t*)c->d_off.p, n,
+                                  (const uint8_t*)c->d_dst.p, dst_len, (uint64_t*)c->d_nhms.p, c->stream));
+    return BLS_OK;
+}
+
+int check_hash_args(const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst, int dst_len) {
+    if (n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (!offsets || (dst_len > 0 && !dst)) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (dst_len < 0 || dst_len > 255) return fail(BLS_ERR_INVALID, "dst_len %d outside 0..255", dst_len);
+    if (n > 0 && offsets[n] > 0 && !msgs) return fail(BLS_ERR_INVALID, "msgs is NULL");
     return BLS_OK;
 }
 
@@ -675,6 +705,42 @@ int bls_verify_batch_device(bls_ctx* ctx, const bls_batch* b, int32_t* results_d
     a.ml_out = b->miller_out;
     a.gt_out = b->gt_out;
     return run_verify(ctx, a);
+}
+
+int bls_neg_hash_to_g1(bls_ctx* ctx, const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst,
+                       int dst_len, uint64_t* out) {
+    if (!ctx || !out) return fail(BLS_ERR_INVALID, "NULL argument");
+    int rc;
+    if ((rc = check_hash_args(msgs, offsets, n, dst, dst_len))) return rc;
+    if (n == 0) return BLS_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CK(cudaSetDevice(ctx->cfg.device));
+    if ((rc = stage_hash(ctx, msgs, offsets, n, dst, dst_len))) return rc;
+    CK(cudaMemcpyAsync(out, ctx->d_nhms.p, (size_t)n * 96, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BLS_OK;
+}
+
+int bls_verify_messages(bls_ctx* ctx, int fmt, const void* sigs, const uint8_t* msgs, const uint32_t* offsets,
+                        const int32_t* pk_ids, int n, const uint8_t* dst, int dst_len, int32_t* results) {
+    if (!ctx || !results) return fail(BLS_ERR_INVALID, "NULL argument");
+    int rc;
+    if ((rc = check_hash_args(msgs, offsets, n, dst, dst_len))) return rc;
+    if (n == 0) return BLS_OK;
+    if (!sigs || !pk_ids) return fail(BLS_ERR_INVALID, "NULL input array");
+    if (fmt != BLS_SIG_AFFINE && fmt != BLS_SIG_COMPRESSED) return fail(BLS_ERR_INVALID, "unknown sig_format %d", fmt);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if ((rc = check_ids(ctx, pk_ids, n))) return rc;
+    CK(cudaSetDevice(ctx->cfg.device));
+    const size_t k = (size_t)n;
+    if ((rc = prepare(ctx, k, fmt, false, false))) return rc;
+    memcpy(ctx->h_sigs.p, sigs, k * (fmt == BLS_SIG_COMPRESSED ? 48 : 96));
+    memcpy(ctx->h_pkidx.p, pk_ids, k * 4);
+    if ((rc = stage_hash(ctx, msgs, offsets, n, dst, dst_len))) return rc;
+    if ((rc = enqueue(ctx, k, fmt, false, false, false, true))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(results, ctx->h_res.p, k * 4);
+    return BLS_OK;
 }
 
 int bls_g1_decompress_status(bls_ctx* ctx, const uint8_t* in, int n, uint64_t* xy, int32_t* status) {

@@ -1,0 +1,218 @@
+// Hash to G1 on the device: RFC 9380 hash_to_curve for BLS12-381 G1 with
+// expand_message_xmd over SHA-256 and the Shallue-van de Woestijne map
+// (section 6.6.1) on y^2 = x^3 + 4, then cofactor clearing by h_eff = 1 - x.
+// The reference's callers hash on the CPU per item with ic_bls12_381's
+// hash_to_curve (ic-integration/patches/ic-gpu-consensus.patch:454-457,
+// ic-bench/src/main.rs:65-76), whose suite maps with SSWU on an 11-isogenous
+// curve; the isogeny's constants are not restated here, so this hash is the
+// SVDW suite of the same RFC and gives different points than ic_bls12_381's.
+// Constants from gen_h2c.py (h2c.inc); the kernel (hash.cu) runs the two maps
+// of a message on two threads.
+#pragma once
+#include "g1.cuh"
+#include "h2c.inc"
+
+namespace bls {
+namespace h2c {
+
+__device__ __forceinline__ uint32_t rotr(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
+
+// SHA-256 compression of one 64-byte block given as 16 big-endian words
+static __device__ __noinline__ void sha256_block(uint32_t* h, const uint32_t* blk) {
+    uint32_t w[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) w[i] = blk[i];
+    uint32_t a = h[0], b = h[1], c = h[2], d = h[3], e = h[4], f = h[5], g = h[6], hh = h[7];
+#pragma unroll
+    for (int t = 0; t < 64; ++t) {
+        uint32_t wt;
+        if (t < 16) {
+            wt = w[t];
+        } else {
+            const uint32_t w15 = w[(t - 15) & 15], w2 = w[(t - 2) & 15];
+            const uint32_t s0 = rotr(w15, 7) ^ rotr(w15, 18) ^ (w15 >> 3);
+            const uint32_t s1 = rotr(w2, 17) ^ rotr(w2, 19) ^ (w2 >> 10);
+            wt = w[t & 15] = w[t & 15] + s0 + w[(t - 7) & 15] + s1;
+        }
+        const uint32_t S1 = rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25);
+        const uint32_t ch = (e & f) ^ (~e & g);
+        const uint32_t t1 = hh + S1 + ch + kSha256K[t] + wt;
+        const uint32_t S0 = rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22);
+        const uint32_t mj = (a & b) ^ (a & c) ^ (b & c);
+        hh = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + S0 + mj;
+    }
+    h[0] += a; h[1] += b; h[2] += c; h[3] += d; h[4] += e; h[5] += f; h[6] += g; h[7] += hh;
+}
+
+// streaming SHA-256, fed byte by byte
+struct Sha256 {
+    uint32_t h[8];
+    uint32_t blk[16];
+    uint32_t fill;    // bytes in blk
+    uint64_t total;   // bytes hashed
+
+    __device__ void init() {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) h[i] = kSha256H0[i];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) blk[i] = 0;
+        fill = 0;
+        total = 0;
+    }
+    __device__ __noinline__ void put(uint32_t byte) {
+        blk[fill >> 2] |= (byte & 0xffu) << (24 - 8 * (fill & 3));
+        ++total;
+        if (++fill == 64) {
+            sha256_block(h, blk);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) blk[i] = 0;
+            fill = 0;
+        }
+    }
+    __device__ void put(const uint8_t* p, uint32_t n) {
+        for (uint32_t i = 0; i < n; ++i) put(p[i]);
+    }
+    // big-endian digest words
+    __device__ void final(uint32_t* out) {
+        const uint64_t bits = total * 8;
+        put(0x80u);
+        while (fill != 56) put(0u);
+        for (int i = 7; i >= 0; --i) put((uint32_t)(bits >> (8 * i)));
+#pragma unroll
+        for (int i = 0; i < 8; ++i) out[i] = h[i];
+    }
+};
+
+// expand_message_xmd(msg, dst, 128) (RFC 9380 section 5.3.1): 32 big-endian words
+__device__ __forceinline__ void expand_xmd_128(const uint8_t* msg, uint32_t len, const uint8_t* dst,
+                                               uint32_t dst_len, uint32_t* out) {
+    Sha256 s;
+    s.init();
+    for (int i = 0; i < 64; ++i) s.put(0u);      // Z_pad
+    s.put(msg, len);
+    s.put(0u);                                   // I2OSP(128, 2)
+    s.put(128u);
+    s.put(0u);                                   // I2OSP(0, 1)
+    s.put(dst, dst_len);
+    s.put(dst_len);
+    uint32_t b0[8], bi[8];
+    s.final(b0);
+    for (uint32_t i = 1; i <= 4; ++i) {
+        s.init();
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t v = i == 1 ? b0[k] : (b0[k] ^ bi[k]);
+            s.put(v >> 24); s.put(v >> 16); s.put(v >> 8); s.put(v);
+        }
+        s.put(i);
+        s.put(dst, dst_len);
+        s.put(dst_len);
+        s.final(bi);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) out[8 * (i - 1) + k] = bi[k];
+    }
+}
+
+// 64 big-endian bytes (16 words) mod p, Montgomery form
+__device__ __forceinline__ fp field_from_be64(const uint32_t* w) {
+    fp hi, lo;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) hi.w[i] = lo.w[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        hi.w[i] = w[7 - i];
+        lo.w[i] = w[15 - i];
+    }
+    return fp_add(fp_mul(lo, fp_rr()), fp_mul(hi, fp_load_u64(kK256)));
+}
+
+static __device__ __noinline__ fp fp_inv0(const fp& a) {   // 0 for 0 (RFC 9380 inv0)
+    return fp_pow_u64(a, kPMinus2, 381);
+}
+
+__device__ __forceinline__ uint32_t sgn0(const fp& a) { return fp_from_mont(a).w[0] & 1u; }
+
+__device__ __forceinline__ fp g_of(const fp& x) { return fp_add(fp_mul(fp_sqr(x), x), fp_four()); }
+
+// the SVDW map, RFC 9380 section 6.6.1 (A = 0, B = 4); square roots by
+// a^((p+1)/4), tested by squaring
+static __device__ __noinline__ void map_svdw(const fp& u, fp& x, fp& y) {
+    const fp one = fp_one();
+    fp tv1 = fp_mul(fp_sqr(u), fp_load_u64(kC1));
+    const fp tv2 = fp_add(one, tv1);
+    tv1 = fp_sub(one, tv1);
+    const fp tv3 = fp_inv0(fp_mul(tv1, tv2));
+    const fp tv4 = fp_mul(fp_mul(fp_mul(u, tv1), tv3), fp_load_u64(kC3));
+    const fp c2 = fp_load_u64(kC2);
+    x = fp_sub(c2, tv4);
+    fp gx = g_of(x);
+    y = fp_sqrt_candidate(gx);
+    if (!fp_eq(fp_sqr(y), gx)) {
+        x = fp_add(c2, tv4);
+        gx = g_of(x);
+        y = fp_sqrt_candidate(gx);
+        if (!fp_eq(fp_sqr(y), gx)) {
+            fp x3 = fp_mul(fp_sqr(tv2), tv3);
+            x3 = fp_mul(fp_sqr(x3), fp_load_u64(kC4));
+            x = fp_add(x3, fp_load_u64(kZ));
+            y = fp_sqrt_candidate(g_of(x));   // a square by construction of Z
+        }
+    }
+    if (sgn0(u) != sgn0(y)) y = fp_neg(y);
+}
+
+// affine (x, y) of a Jacobian point; false for the identity
+__device__ __forceinline__ bool to_affine(const g1j& p, fp& x, fp& y) {
+    if (fp_is_zero(p.Z)) return false;
+    const fp zi = fp_inv0(p.Z), zi2 = fp_sqr(zi);
+    x = fp_mul(p.X, zi2);
+    y = fp_mul(p.Y, fp_mul(zi2, zi));
+    return true;
+}
+
+// p + q, both Jacobian (add-2007-bl), exceptional cases handled
+static __device__ __noinline__ g1j g1j_add(const g1j& p, const g1j& q) {
+    if (fp_is_zero(p.Z)) return q;
+    if (fp_is_zero(q.Z)) return p;
+    const fp Z1Z1 = fp_sqr(p.Z), Z2Z2 = fp_sqr(q.Z);
+    const fp U1 = fp_mul(p.X, Z2Z2), U2 = fp_mul(q.X, Z1Z1);
+    const fp S1 = fp_mul(fp_mul(p.Y, q.Z), Z2Z2), S2 = fp_mul(fp_mul(q.Y, p.Z), Z1Z1);
+    const fp H = fp_sub(U2, U1);
+    fp rr = fp_sub(S2, S1);
+    if (fp_is_zero(H)) {
+        if (fp_is_zero(rr)) return g1j_dbl(p);
+        return {fp_one(), fp_one(), fp_zero()};
+    }
+    fp I = fp_add(H, H);
+    I = fp_sqr(I);
+    const fp J = fp_mul(H, I);
+    rr = fp_add(rr, rr);
+    const fp V = fp_mul(U1, I);
+    g1j r;
+    r.X = fp_sub(fp_sub(fp_sqr(rr), J), fp_add(V, V));
+    const fp SJ = fp_mul(S1, J);
+    r.Y = fp_sub(fp_mul(rr, fp_sub(V, r.X)), fp_add(SJ, SJ));
+    r.Z = fp_mul(fp_sub(fp_sub(fp_sqr(fp_add(p.Z, q.Z)), Z1Z1), Z2Z2), H);
+    return r;
+}
+
+// -H(msg) from the two mapped points (affine), as affine Montgomery (x, y);
+// the identity as x = 0, y = R mod p.  Q = P0 + P1 stays Jacobian through the
+// cofactor clearing [h_eff] Q; one inversion at the end.
+static __device__ __noinline__ void neg_clear(const fp& x0, const fp& y0, const fp& x1, const fp& y1, fp& ox,
+                                              fp& oy) {
+    const g1j q = g1j_add_affine(g1j{x0, y0, fp_one()}, x1, y1);
+    g1j r = q;
+    for (int i = 62; i >= 0; --i) {
+        r = g1j_dbl(r);
+        if ((kHEff >> i) & 1) r = g1j_add(r, q);
+    }
+    fp rx, ry;
+    ox = fp_zero();
+    oy = fp_one();
+    if (!to_affine(r, rx, ry)) return;
+    ox = rx;
+    oy = fp_neg(ry);
+}
+
+}  // namespace h2c
+}  // namespace bls

@@ -33,6 +33,8 @@ struct VerifyArgs {
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
+cudaError_t launch_neg_hash_to_g1(const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst,
+                                  int dst_len, uint64_t* out, cudaStream_t s);
 cudaError_t launch_g2_decompress(const uint8_t* in, int n, uint64_t* q, int32_t* status, uint8_t* identity,
                                  cudaStream_t s);
 cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStream_t s);

@@ -194,7 +194,7 @@ def _items(rng, keys, key_of_item, corrupt):
     h_checked = h_signed.copy()
     if flip.any():
         h_checked[flip] = hash_to_g1([checked[i] for i in range(n) if flip[i]])
-    return {"sigs": sigs, "nhms": g1_neg(h_checked), "pk_index": pk_index, "expect": expect}
+    return {"sigs": sigs, "nhms": g1_neg(h_checked), "pk_index": pk_index, "expect": expect, "msgs": checked}
 
 
 def config_plain(n=64, seed=1):

@@ -255,6 +255,23 @@ int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64_t* neg_hms
                                   const uint64_t* pk_tables, const int32_t* pk_index, int32_t* results, int n,
                                   int lanes_per_pairing, void* stream);
 
+/* -H(m_i) for n messages on the GPU, in the neg_hms layout (12 x uint64 each,
+ * affine Montgomery).  H is RFC 9380 hash_to_curve to G1 with
+ * expand_message_xmd over SHA-256 and domain `dst` (0..255 bytes), using the
+ * Shallue-van de Woestijne map (RFC 9380 section 6.6.1) and h_eff = 1 - x:
+ * the RFC's SVDW suite.  ic_bls12_381's hash_to_curve uses the SSWU suite,
+ * whose points differ, so callers that must match it keep hashing on the CPU.
+ * msgs: the messages back to back; offsets: n + 1 byte offsets, offsets[0] = 0,
+ * non-decreasing (message i is msgs[offsets[i] .. offsets[i+1])). */
+int bls_neg_hash_to_g1(bls_ctx* ctx, const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst,
+                       int dst_len, uint64_t* out);
+/* Verify n signatures against messages: -H(m_i) as bls_neg_hash_to_g1 computes
+ * it on the GPU, straight into the verify launch's input.  sig_format and
+ * results as in bls_verify_batch. */
+int bls_verify_messages(bls_ctx* ctx, int sig_format, const void* sigs, const uint8_t* msgs,
+                        const uint32_t* offsets, const int32_t* pk_ids, int n, const uint8_t* dst, int dst_len,
+                        int32_t* results);
+
 /* Decode n compressed G1 points: status[i] (BLS_ST_*), xy[i] 12 x uint64
  * (identity: x = 0, y = R mod p; failures: zeros). */
 int bls_g1_decompress_status(bls_ctx* ctx, const uint8_t* compressed, int n, uint64_t* xy, int32_t* status);

@@ -1,0 +1,127 @@
+"""Hash to G1 on the GPU (bls_neg_hash_to_g1, bls_verify_messages): RFC 9380
+hash_to_curve with expand_message_xmd over SHA-256 and the SVDW map.  The
+reference's callers hash on the CPU (ic-integration/patches/
+ic-gpu-consensus.patch:454-457); the device constants are derived by
+icp-gpu_b200/csrc/gen_h2c.py and checked here against the oracle and hashlib,
+the device outputs against the oracle's hash_to_g1 and the workload's C++ hash."""
+import hashlib
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import bls_ref as B
+import bls_gpu as G
+import cpu as C
+import workload_py as W
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "icp-gpu_b200", "csrc"))
+import gen_h2c as H  # noqa: E402
+
+
+# ------------------------------------------------------------------ CPU side
+
+def _sha256(msg, K, H0):
+    """FIPS 180-4 SHA-256 written out with the generator's constants."""
+    def rotr(x, n):
+        return ((x >> n) | (x << (32 - n))) & 0xffffffff
+    m = bytes(msg) + b"\x80" + bytes((55 - len(msg)) % 64) + (8 * len(msg)).to_bytes(8, "big")
+    h = list(H0)
+    for blk in range(0, len(m), 64):
+        w = [int.from_bytes(m[blk + 4 * i:blk + 4 * i + 4], "big") for i in range(16)]
+        for t in range(16, 64):
+            s0 = rotr(w[t - 15], 7) ^ rotr(w[t - 15], 18) ^ (w[t - 15] >> 3)
+            s1 = rotr(w[t - 2], 17) ^ rotr(w[t - 2], 19) ^ (w[t - 2] >> 10)
+            w.append((w[t - 16] + s0 + w[t - 7] + s1) & 0xffffffff)
+        a, b, c, d, e, f, g, hh = h
+        for t in range(64):
+            t1 = (hh + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + K[t] + w[t]) & 0xffffffff
+            t2 = ((rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c))) & 0xffffffff
+            hh, g, f, e, d, c, b, a = g, f, e, (d + t1) & 0xffffffff, c, b, a, (t1 + t2) & 0xffffffff
+        h = [(x + y) & 0xffffffff for x, y in zip(h, (a, b, c, d, e, f, g, hh))]
+    return b"".join(x.to_bytes(4, "big") for x in h)
+
+
+def test_sha256_constants_against_hashlib():
+    for n in (0, 1, 55, 56, 63, 64, 65, 200):
+        msg = bytes((7 * i + n) & 0xff for i in range(n))
+        assert _sha256(msg, H.SHA256_K, H.SHA256_H0) == hashlib.sha256(msg).digest()
+
+
+def test_map_constants_match_oracle():
+    assert H.SVDW_Z == B.SVDW_Z
+    assert (H.SVDW_C1, H.SVDW_C2, H.SVDW_C3, H.SVDW_C4) == (B.SVDW_C1, B.SVDW_C2, B.SVDW_C3, B.SVDW_C4)
+    assert H.H_EFF == B.H_EFF_G1
+    assert H.K256 == (1 << 256) * (1 << 768) % B.P
+
+
+def test_header_current():
+    """h2c.inc is what the generator writes now."""
+    path = os.path.join(os.path.dirname(H.__file__), "h2c.inc")
+    before = open(path).read()
+    H.emit()
+    assert open(path).read() == before
+
+
+# ------------------------------------------------------------------ GPU side
+
+@pytest.fixture(scope="module")
+def ctx():
+    G.init()
+    with G.Context() as c:
+        yield c
+
+
+def _oracle_neg(msg, dst):
+    return np.array(B.g1_to_mont_u64(B.g1_neg(B.hash_to_g1(msg, dst))), dtype=np.uint64)
+
+
+@pytest.mark.gpu
+def test_hash_matches_oracle_lengths(ctx):
+    dst = W.DST
+    msgs = [bytes((3 * i + n) & 0xff for i in range(n)) for n in (0, 1, 31, 32, 55, 56, 63, 64, 65, 119, 120, 200, 1000)]
+    got = ctx.neg_hash_to_g1(msgs, dst)
+    for i, m in enumerate(msgs):
+        assert (got[i] == _oracle_neg(m, dst)).all(), len(m)
+
+
+@pytest.mark.gpu
+def test_hash_domains(ctx):
+    msg = [b"abc"]
+    for dst in (b"X", b"QUUX-V01-CS02-with-BLS12381G1_XMD:SHA-256_SVDW_RO_", bytes(range(255))):
+        assert (ctx.neg_hash_to_g1(msg, dst)[0] == _oracle_neg(msg[0], dst)).all()
+
+
+@pytest.mark.gpu
+def test_hash_matches_workload_batch(ctx):
+    rng = W.SplitMix64(77)
+    msgs = [rng.msg() for _ in range(512)]
+    want = W.WL.g1_neg(W.WL.hash_to_g1(msgs))
+    assert (ctx.neg_hash_to_g1(msgs, W.DST) == want).all()
+
+
+@pytest.mark.gpu
+def test_verify_messages(ctx, golden):
+    wl = W.plain_config(n=64, seed=5)
+    ids = [ctx.register_pk_coeffs(t) for t in wl["pk_tabs"]]
+    res = ctx.verify_messages(wl["sigs"], wl["msgs"], ids, W.DST)
+    assert (res == wl["expect"]).all()
+    assert (res == ctx.verify(wl["sigs"], wl["nhms"], ids)).all()
+    enc = W.WL.g1_compress(wl["sigs"])
+    assert (ctx.verify_messages(enc.tobytes(), wl["msgs"], ids, W.DST, compressed=True) == wl["expect"]).all()
+    # a wrong domain rejects every item
+    assert (ctx.verify_messages(wl["sigs"], wl["msgs"], ids, b"OTHER") == 0).all()
+
+
+@pytest.mark.gpu
+def test_hash_argument_checks(ctx):
+    L = ctx.lib
+    buf, off = G.pack_messages([b"ab", b"c"])
+    out = np.zeros((2, 12), dtype=np.uint64)
+    bad = off.copy()
+    bad[1], bad[2] = 3, 2                                         # decreasing
+    assert L.bls_neg_hash_to_g1(ctx.h, buf.ctypes.data, bad.ctypes.data, 2, None, 0, out.ctypes.data) == G.BLS_ERR_INVALID
+    d = np.zeros(256, dtype=np.uint8)
+    assert L.bls_neg_hash_to_g1(ctx.h, buf.ctypes.data, off.ctypes.data, 2, d.ctypes.data, 256,
+                                out.ctypes.data) == G.BLS_ERR_INVALID

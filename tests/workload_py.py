@@ -20,7 +20,7 @@ def plain_config(n=64, seed=1):
     c = WL.config_plain(n, seed)
     return {
         "sigs": c["sigs"], "nhms": c["nhms"], "pk_tabs": c["pk_tables"], "pk_affine": c["pk_affine"],
-        "expect": c["expect"], "sig_points": [B.g1_from_mont_u64(s) for s in c["sigs"]],
+        "expect": c["expect"], "sig_points": [B.g1_from_mont_u64(s) for s in c["sigs"]], "msgs": c["msgs"],
     }
 
 
