@@ -306,11 +306,12 @@ def run_gpu(args):
     e2e_s = max_over_ranks(pg, sum(e2e_times), dev)
     e2e_value = whole_job_rate(N_ITEMS, world, args.steps, e2e_s)
 
-    batching = serving = ingest = hashing = None
+    batching = serving = ingest = hashing = rlc = None
     if not args.no_extras:
         sizes = [int(v) for v in args.ingest_keys.split(",") if int(v) > 0]
         ingest = [run_ingest(G, WL, local, args.lanes, k) for k in sizes] or None
         hashing = run_hash(G, WL, ctx, wl, pk_ids)
+        rlc = run_rlc(G, WL, ctx, wl, pk_ids, n=args.rlc_items) if args.rlc_items > 0 else None
         batching = run_batching(G, WL, ctx, ids)
         if args.serve_seconds > 0:
             serving = run_serving(G, WL, ctx, args.serve_seconds, slots=args.serve_slots,
@@ -353,6 +354,8 @@ def run_gpu(args):
             result["ingest"] = ingest
         if hashing:
             result["hash"] = hashing
+        if rlc:
+            result["rlc"] = rlc
         if batching:
             result["batching"] = batching
         if serving:
@@ -451,6 +454,37 @@ def run_hash(G, WL, ctx, wl, pk_ids, reps=3):
             "cpu_hash_per_s": round(n / t_cpu_hash, 1), "cpu_threads": WL.nthreads()}
 
 
+def run_rlc(G, WL, ctx, wl4096, pk_ids4096, n=65536, reps=3):
+    """Random-linear-combination batches (bls_verify_batch_rlc) from host
+    buffers: an all-valid batch (the corrupted items of a keyset-n-40 draw
+    removed) against the same batch item by item (bls_verify_batch); and the
+    headline 4,096-item workload, whose 1-in-8 corrupted items make the combined
+    check fail, to show the cost of the fallback (host-timed, best of reps)."""
+    wl = WL.config_keyset(n, N_KEYS, seed=SEED + 5)
+    keep = np.nonzero(wl["expect"] == 1)[0]
+    ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)[wl["pk_index"][keep]]
+    sigs, nhms = wl["sigs"][keep], wl["nhms"][keep]
+
+    def best(fn):
+        t, out = 1e30, None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = fn()
+            t = min(t, time.perf_counter() - t0)
+        return t, out
+    t_item, r_item = best(lambda: ctx.verify(sigs, nhms, ids))
+    t_rlc, (r_rlc, comb) = best(lambda: ctx.verify_rlc(sigs, nhms, ids))
+    assert comb == 1 and (r_rlc == 1).all() and (r_item == 1).all(), "all-valid batch not accepted"
+    t_fb, (r_fb, comb_fb) = best(lambda: ctx.verify_rlc(wl4096["sigs"], wl4096["nhms"], pk_ids4096))
+    assert comb_fb == 0 and (r_fb == wl4096["expect"]).all(), "fallback results differ"
+    t_fb_item, _ = best(lambda: ctx.verify(wl4096["sigs"], wl4096["nhms"], pk_ids4096))
+    m = len(keep)
+    return {"items": m, "keys": N_KEYS, "api": "bls_verify_batch_rlc vs bls_verify_batch (host buffers)",
+            "per_item_verifies_per_s": round(m / t_item, 1), "rlc_verifies_per_s": round(m / t_rlc, 1),
+            "speedup": round(t_item / t_rlc, 2), "rlc_ms": round(t_rlc * 1e3, 2),
+            "fallback_4096_ms": round(t_fb * 1e3, 2), "per_item_4096_ms": round(t_fb_item * 1e3, 2)}
+
+
 def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192):
     """Serving workload: seeded Poisson stream of requests (sizes log-uniform in
     [1, 512]) over a pool of 40 resident keys, through the continuous-batching
@@ -539,6 +573,7 @@ def main():
     ap.add_argument("--lanes", type=int, default=6, help="lanes per verification (6: Fp2-lane kernel; 1, 2, 4, 8)")
     ap.add_argument("--ingest-keys", default="1024,16384",
                     help="comma-separated key counts ingested compressed on the GPU (0 = skip)")
+    ap.add_argument("--rlc-items", type=int, default=65536, help="random-linear-combination batch draw (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the serving stream (0 = skip)")
     ap.add_argument("--serve-slots", type=int, default=6, help="serving: launches in flight")
     ap.add_argument("--serve-max-batch", type=int, default=1480, help="serving: items per launch")

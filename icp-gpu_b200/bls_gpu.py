@@ -107,6 +107,7 @@ def lib():
         L.bls_ctx_stream.restype = P
         L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
         L.bls_neg_hash_to_g1.argtypes = [P, P, P, I, P, I, P]
+        L.bls_verify_batch_rlc.argtypes = [P, ctypes.POINTER(Batch), P, P, ctypes.POINTER(I), P]
         L.bls_verify_messages.argtypes = [P, I, P, P, P, P, I, P, I, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
         L.bls_verify_compressed_noalloc.argtypes = [P, P, P, P, P, P, I, I, P]
@@ -310,6 +311,28 @@ class Context:
         b = Batch(n, SIG_COMPRESSED if compressed else SIG_AFFINE, _ptr(s), _ptr(nhms), _ptr(ids), _ptr(ml), _ptr(gt))
         self._check(self.lib.bls_verify_batch(self.h, ctypes.byref(b), _ptr(res)), "bls_verify_batch")
         return (res, ml, gt) if want_values else res
+
+    def verify_rlc(self, sigs, neg_hms, pk_ids, compressed=False, scalars=None, want_agg=False):
+        """Random-linear-combination batch verification: (results, combined[, agg])."""
+        nhms = _u64(neg_hms, 12)
+        n = nhms.shape[0]
+        if compressed:
+            s = np.ascontiguousarray(np.frombuffer(bytes(sigs), dtype=np.uint8) if not isinstance(sigs, np.ndarray)
+                                     else sigs, dtype=np.uint8).reshape(-1)
+            assert s.size == 48 * n
+        else:
+            s = _u64(sigs, 12)
+            assert s.shape[0] == n
+        ids = np.ascontiguousarray(pk_ids, dtype=np.int32).reshape(-1)
+        assert ids.size == n
+        r = None if scalars is None else np.ascontiguousarray(scalars, dtype=np.uint64).reshape(-1)
+        res = np.zeros(n, dtype=np.int32)
+        comb = ctypes.c_int(0)
+        agg = np.zeros((1 + len(set(ids.tolist())), 12), dtype=np.uint64) if want_agg else None
+        b = Batch(n, SIG_COMPRESSED if compressed else SIG_AFFINE, _ptr(s), _ptr(nhms), _ptr(ids), None, None)
+        self._check(self.lib.bls_verify_batch_rlc(self.h, ctypes.byref(b), _ptr(r), _ptr(res), ctypes.byref(comb),
+                                                  _ptr(agg)), "bls_verify_batch_rlc")
+        return (res, comb.value, agg) if want_agg else (res, comb.value)
 
     def verify_device(self, n, sigs_ptr, nhms_ptr, ids_ptr, res_ptr, compressed=False, ml_ptr=None, gt_ptr=None):
         """Enqueue a verify on device-resident arrays (raw device pointers)."""

@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,8 @@
 #include <mutex>
 #include <string>
 #include <vector>
+
+#include <sys/random.h>
 
 #include "internal.h"
 
@@ -79,6 +82,7 @@ struct bls_ctx {
     // per-call scratch
     DevBuf d_sigs, d_nhms, d_pkidx, d_res, d_ml, d_gt, d_pk_items, d_g2_call, d_in, d_xy, d_st, d_work;
     DevBuf d_msg, d_off, d_dst;  // message bytes, offsets and domain of a hash
+    DevBuf d_rlc;                // scratch of a random-linear-combination batch
     HostBuf h_sigs, h_nhms, h_pkidx, h_res;
 
     // persistent batched launch captured as a CUDA graph, valid while the
@@ -157,7 +161,7 @@ struct bls_ctx {
     void release() {
         drop_graph();
         for (DevBuf* b : {&d_sigs, &d_nhms, &d_pkidx, &d_res, &d_ml, &d_gt, &d_pk_items, &d_g2_call, &d_in,
-                          &d_xy, &d_st, &d_work, &d_msg, &d_off, &d_dst})
+                          &d_xy, &d_st, &d_work, &d_msg, &d_off, &d_dst, &d_rlc})
             if (b->p) cudaFree(b->p);
         for (HostBuf* b : {&h_sigs, &h_nhms, &h_pkidx, &h_res})
             if (b->p) cudaFreeHost(b->p);
@@ -705,6 +709,152 @@ int bls_verify_batch_device(bls_ctx* ctx, const bls_batch* b, int32_t* results_d
     a.ml_out = b->miller_out;
     a.gt_out = b->gt_out;
     return run_verify(ctx, a);
+}
+
+// Random-linear-combination batch: see rlc.cu.  Host side: scalars, the items
+// grouped by key (counting sort), tiles of at most kRlcTile items of one key.
+int bls_verify_batch_rlc(bls_ctx* ctx, const bls_batch* b, const uint64_t* scalars, int32_t* results,
+                         int* combined, uint64_t* agg_out) {
+    constexpr int kRlcTile = 1024;
+    if (!ctx || !b || !results) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (b->n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (combined) *combined = 0;
+    if (b->n == 0) {
+        if (combined) *combined = 1;
+        return BLS_OK;
+    }
+    if (!b->sigs || !b->neg_hms || !b->pk_ids) return fail(BLS_ERR_INVALID, "NULL input array");
+    if (b->miller_out || b->gt_out) return fail(BLS_ERR_INVALID, "per-item Miller / Gt values need bls_verify_batch");
+    const int fmt = b->sig_format;
+    if (fmt != BLS_SIG_AFFINE && fmt != BLS_SIG_COMPRESSED) return fail(BLS_ERR_INVALID, "unknown sig_format %d", fmt);
+    const size_t n = (size_t)b->n;
+    std::vector<uint64_t> r(n);
+    if (scalars) {
+        for (size_t i = 0; i < n; ++i)
+            if (!scalars[i]) return fail(BLS_ERR_INVALID, "scalar %zu is zero", i);
+        memcpy(r.data(), scalars, n * 8);
+    } else {
+        uint8_t* p = (uint8_t*)r.data();
+        size_t got = 0;
+        while (got < n * 8) {
+            ssize_t k = getrandom(p + got, n * 8 - got, 0);
+            if (k < 0) return fail(BLS_ERR_INVALID, "getrandom failed");
+            got += (size_t)k;
+        }
+        for (auto& v : r)
+            if (!v) v = 1;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int rc;
+    if ((rc = check_ids(ctx, b->pk_ids, b->n))) return rc;
+    CK(cudaSetDevice(ctx->cfg.device));
+    // items grouped by key; key slots in increasing id; tiles of one key
+    std::vector<int32_t> start(ctx->n_pks + 1, 0), order(n), keys, key_tile, tiles;
+    for (size_t i = 0; i < n; ++i) start[b->pk_ids[i] + 1]++;
+    for (int k = 0; k < ctx->n_pks; ++k) start[k + 1] += start[k];
+    {
+        std::vector<int32_t> pos(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < n; ++i) order[pos[b->pk_ids[i]]++] = (int32_t)i;
+    }
+    for (int k = 0; k < ctx->n_pks; ++k) {
+        if (start[k + 1] == start[k]) continue;
+        key_tile.push_back((int32_t)(tiles.size() / 3));
+        for (int a = start[k]; a < start[k + 1]; a += kRlcTile) {
+            tiles.push_back(a);
+            tiles.push_back(std::min(a + kRlcTile, start[k + 1]));
+            tiles.push_back((int32_t)keys.size());
+        }
+        keys.push_back(k);
+    }
+    key_tile.push_back((int32_t)(tiles.size() / 3));
+    const int nkeys = (int)keys.size(), ntiles = (int)(tiles.size() / 3);
+    // scratch: pts, partials, aggregates, scalars, order, tiles, key_tile, keys, bad, results, counters
+    auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t o_pts = 0, o_part = o_pts + al(n * 288), o_sig = o_part + al((size_t)ntiles * 288),
+                 o_nhm = o_sig + al((size_t)nkeys * 96), o_r = o_nhm + al((size_t)nkeys * 96), o_ord = o_r + al(n * 8),
+                 o_til = o_ord + al(n * 4), o_kt = o_til + al(tiles.size() * 4),
+                 o_key = o_kt + al(key_tile.size() * 4), o_bad = o_key + al((size_t)nkeys * 4),
+                 o_res = o_bad + al(n * 2), o_cnt = o_res + al((size_t)nkeys * 4), total = o_cnt + 256;
+    if ((rc = prepare(ctx, n, fmt, false, false)) || (rc = ctx->grow(ctx->d_rlc, total)) ||
+        (rc = ctx->grow(ctx->d_gt, (size_t)nkeys * 576)))
+        return rc;
+    uint8_t* base = (uint8_t*)ctx->d_rlc.p;
+    const size_t sig_bytes = n * (fmt == BLS_SIG_COMPRESSED ? 48 : 96);
+    memcpy(ctx->h_sigs.p, b->sigs, sig_bytes);
+    memcpy(ctx->h_nhms.p, b->neg_hms, n * 96);
+    memcpy(ctx->h_pkidx.p, b->pk_ids, n * 4);
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_sigs.p, ctx->h_sigs.p, sig_bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_nhms.p, ctx->h_nhms.p, n * 96, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(base + o_r, r.data(), n * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(base + o_ord, order.data(), n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(base + o_til, tiles.data(), tiles.size() * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(base + o_kt, key_tile.data(), key_tile.size() * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(base + o_key, keys.data(), (size_t)nkeys * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(base + o_cnt, 0, 8, st));
+    bls::RlcArgs ra{};
+    if (fmt == BLS_SIG_COMPRESSED) {
+        CK(bls::launch_g1_decompress((const uint8_t*)ctx->d_sigs.p, b->n, (uint64_t*)ctx->d_xy.p,
+                                     (int32_t*)ctx->d_st.p, st));
+        ra.sig_xy = (const uint64_t*)ctx->d_xy.p;
+        ra.status = (const int32_t*)ctx->d_st.p;
+    } else {
+        ra.sig_xy = (const uint64_t*)ctx->d_sigs.p;
+        ra.check_sig = 1;
+    }
+    ra.nhms = (const uint64_t*)ctx->d_nhms.p;
+    ra.r = (const uint64_t*)(base + o_r);
+    ra.n = b->n;
+    ra.pts = (uint32_t*)(base + o_pts);
+    ra.bad = base + o_bad;
+    ra.counters = (int*)(base + o_cnt);
+    ra.order = (const int32_t*)(base + o_ord);
+    ra.tiles = (const int32_t*)(base + o_til);
+    ra.ntiles = ntiles;
+    ra.partials = (uint32_t*)(base + o_part);
+    ra.key_tile = (const int32_t*)(base + o_kt);
+    ra.nkeys = nkeys;
+    ra.agg_sigs = (uint64_t*)(base + o_sig);
+    ra.agg_nhms = (uint64_t*)(base + o_nhm);
+    CK(bls::launch_rlc(ra, st));
+    // one verify item per key: Miller loops of the sums and their final exponentiations
+    bls::VerifyArgs a{};
+    a.sigs = ra.agg_sigs;
+    a.nhms = ra.agg_nhms;
+    a.g2 = ctx->d_g2;
+    a.pk_tables = ctx->d_pk;
+    ctx->set_norm(a);
+    a.pk_index = (const int32_t*)(base + o_key);
+    a.pk_identity = ctx->d_pk_inf;
+    a.n = nkeys;
+    a.results = (int32_t*)(base + o_res);
+    a.gt_out = (uint64_t*)ctx->d_gt.p;
+    if ((rc = run_verify(ctx, a))) return rc;
+    CK(bls::launch_gt_product((uint64_t*)ctx->d_gt.p, nkeys, ra.counters, st));
+    int cnt[2] = {0, 0};
+    CK(cudaMemcpyAsync(cnt, ra.counters, 8, cudaMemcpyDeviceToHost, st));
+    if (agg_out) {
+        CK(cudaMemcpyAsync(agg_out, ra.agg_sigs, 96, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(agg_out + 12, ra.agg_nhms, (size_t)nkeys * 96, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    const bool ok = cnt[0] == 1 && cnt[1] == 0;
+    if (ok) {
+        if (fmt == BLS_SIG_COMPRESSED) {
+            CK(cudaMemcpyAsync(results, ctx->d_st.p, n * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (size_t i = 0; i < n; ++i) results[i] = results[i] ? -results[i] : BLS_ACCEPT;
+        } else {
+            for (size_t i = 0; i < n; ++i) results[i] = BLS_ACCEPT;
+        }
+    } else {
+        // the per-item path on the staged inputs
+        if ((rc = enqueue(ctx, n, fmt, false, false, false))) return rc;
+        CK(cudaStreamSynchronize(st));
+        memcpy(results, ctx->h_res.p, n * 4);
+    }
+    if (combined) *combined = ok ? 1 : 0;
+    return BLS_OK;
 }
 
 int bls_neg_hash_to_g1(bls_ctx* ctx, const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst,

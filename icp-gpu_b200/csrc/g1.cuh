@@ -96,6 +96,32 @@ static __device__ __noinline__ g1j g1j_add_affine(const g1j& p, const fp& qx, co
     return r;
 }
 
+// p + q, both Jacobian (add-2007-bl), exceptional cases handled
+static __device__ __noinline__ g1j g1j_add(const g1j& p, const g1j& q) {
+    if (fp_is_zero(p.Z)) return q;
+    if (fp_is_zero(q.Z)) return p;
+    const fp Z1Z1 = fp_sqr(p.Z), Z2Z2 = fp_sqr(q.Z);
+    const fp U1 = fp_mul(p.X, Z2Z2), U2 = fp_mul(q.X, Z1Z1);
+    const fp S1 = fp_mul(fp_mul(p.Y, q.Z), Z2Z2), S2 = fp_mul(fp_mul(q.Y, p.Z), Z1Z1);
+    const fp H = fp_sub(U2, U1);
+    fp rr = fp_sub(S2, S1);
+    if (fp_is_zero(H)) {
+        if (fp_is_zero(rr)) return g1j_dbl(p);
+        return {fp_one(), fp_one(), fp_zero()};
+    }
+    fp I = fp_add(H, H);
+    I = fp_sqr(I);
+    const fp J = fp_mul(H, I);
+    rr = fp_add(rr, rr);
+    const fp V = fp_mul(U1, I);
+    g1j r;
+    r.X = fp_sub(fp_sub(fp_sqr(rr), J), fp_add(V, V));
+    const fp SJ = fp_mul(S1, J);
+    r.Y = fp_sub(fp_mul(rr, fp_sub(V, r.X)), fp_add(SJ, SJ));
+    r.Z = fp_mul(fp_sub(fp_sub(fp_sqr(fp_add(p.Z, q.Z)), Z1Z1), Z2Z2), H);
+    return r;
+}
+
 // phi(P) == -[x^2] P for an affine curve point P (not the identity)
 static __device__ __noinline__ bool g1_in_subgroup(const fp& x, const fp& y) {
     // x^2 = 0xac45a4010001a402_0000000100000000 (128 bits, 17 set)

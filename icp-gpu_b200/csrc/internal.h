@@ -32,6 +32,29 @@ struct VerifyArgs {
 };
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
+
+// random-linear-combination batch check (rlc.cu), device pointers
+struct RlcArgs {
+    const uint64_t* sig_xy;   // n x 12 u64 affine signatures (decoded when the input was compressed)
+    const int32_t* status;    // n decode statuses, or NULL
+    const uint64_t* nhms;     // n x 12 u64
+    const uint64_t* r;        // n nonzero scalars
+    int n;
+    int check_sig;            // check the signatures too (affine input; the decoder checked compressed ones)
+    uint32_t* pts;            // n x 72 words scratch: [r] sig, [r] nhm (Jacobian)
+    uint8_t* bad;             // n x 2: a signature / nhm that failed its checks
+    int* counters;            // [0] combined check is one, [1] points that failed their checks (zeroed)
+    const int32_t* order;     // n item ids, grouped by key
+    const int32_t* tiles;     // ntiles x 3: [start, end) in order, key slot
+    int ntiles;
+    uint32_t* partials;       // ntiles x 72 words scratch
+    const int32_t* key_tile;  // nkeys + 1: first tile of each key slot
+    int nkeys;
+    uint64_t* agg_sigs;       // nkeys x 12 u64: verify items, pair 1
+    uint64_t* agg_nhms;       // nkeys x 12 u64: verify items, pair 2
+};
+cudaError_t launch_rlc(const RlcArgs& a, cudaStream_t s);
+cudaError_t launch_gt_product(uint64_t* gt, int n, int* counters, cudaStream_t s);
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
 cudaError_t launch_neg_hash_to_g1(const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst,
                                   int dst_len, uint64_t* out, cudaStream_t s);

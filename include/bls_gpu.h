@@ -255,6 +255,26 @@ int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64_t* neg_hms
                                   const uint64_t* pk_tables, const int32_t* pk_index, int32_t* results, int n,
                                   int lanes_per_pairing, void* stream);
 
+/* Random-linear-combination batch verification (opt-in): one combined check
+ *   e(sum r_i sig_i, G2) * prod_k e(sum_{pk_i = k} r_i (-H(m_i)), pk_k) == 1
+ * over random nonzero r_i, with one final exponentiation for the whole
+ * batch.  When it holds, every item is accepted (results[i] = BLS_ACCEPT, or
+ * -status for a compressed signature that failed to decode); the chance that
+ * it holds while some item is invalid is at most 2^-64.  When it fails, or any
+ * point is off the curve, non-canonical or outside G1 (the combination is
+ * sound only in G1), the batch is verified item by item, so results always
+ * equal bls_verify_batch's up to that chance.  scalars: n nonzero 64-bit
+ * values s_i (tests), or NULL to draw them from the operating system; the
+ * scalar of item i is r_i = (s_i mod 2^32) + lambda (s_i >> 32) mod r, lambda
+ * = -x^2 the eigenvalue of the G1 endomorphism (x, y) -> (beta x, y), so a
+ * multiplication needs 32 doublings and 2^64 scalars remain distinct.  combined (optional): 1 when
+ * the combined check accepted the batch.  agg_out (optional, 12 x (1 + K)
+ * uint64, K = distinct keys): the signature sum, then each key's sum in
+ * increasing key id, affine (identity: x = 0, y = R mod p).  batch->miller_out
+ * and gt_out must be NULL. */
+int bls_verify_batch_rlc(bls_ctx* ctx, const bls_batch* batch, const uint64_t* scalars, int32_t* results,
+                         int* combined, uint64_t* agg_out);
+
 /* -H(m_i) for n messages on the GPU, in the neg_hms layout (12 x uint64 each,
  * affine Montgomery).  H is RFC 9380 hash_to_curve to G1 with
  * expand_message_xmd over SHA-256 and domain `dst` (0..255 bytes), using the
