@@ -124,65 +124,68 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
             f2::acc_add_hi(accX, x1, neg);
             continue;
         }
-        // operands of products 0 and 1: (A0, B0), (A1, B1); KARA's product 2 is (A0 + A1, B0 + B1)
-        uint32_t A0[12], A1[12], B0[12], B1[12];
-        load_fp(A0, sm, xs, 0);
-        load_fp(A1, sm, xs, 1);
-        if (kind == f2::kKara) {
-            load_fp(B0, sm, ys, 0);
-            load_fp(B1, sm, ys, 1);
-            if (xi) {                       // X = xi X = (x0 - x1 + 3p, x0 + x1)
-                uint32_t s[12];
-                f2::add12(s, A0, A1);
-                f2::add3p_sub(A0, A0, A1);
-#pragma unroll
-                for (int i = 0; i < 12; ++i) A1[i] = s[i];
-            }
-            if (dbl) {
-                f2::dbl12(B0);
-                f2::dbl12(B1);
-            }
-        } else if (kind == f2::kSqr) {
-            f2::add3p_sub(B0, A0, A1);      // x0 - x1 + 3p
-#pragma unroll
-            for (int i = 0; i < 12; ++i) B1[i] = A1[i];
-            uint32_t s[12];
-            f2::add12(s, A0, A1);
-            f2::dbl12(A0);
-#pragma unroll
-            for (int i = 0; i < 12; ++i) {
-                A1[i] = A0[i];              // 2 x0
-                A0[i] = s[i];               // x0 + x1
-            }
-        } else if (kind == f2::kFpMul) {
-            load_fp(B0, sm, ys, yim);
-#pragma unroll
-            for (int i = 0; i < 12; ++i) B1[i] = B0[i];
-        } else {                            // NORM
-#pragma unroll
-            for (int i = 0; i < 12; ++i) {
-                B0[i] = A0[i];
-                B1[i] = A1[i];
-            }
-        }
-        // coefficients in {-1, 0, 1}: bit 0 nonzero, bit 1 negative (4 bits per product).
-        // Products (A0, B0), (A1, B1), then KARA's (A0 + A1, B0 + B1) with the sums
-        // formed in place: no operand copies stay live beside the accumulators.
+        // coefficients in {-1, 0, 1} of product j: bit 0 nonzero, bit 1 negative;
+        // (cw >> 4j) for component 0, (cw >> 4(3 + j)) for component 1
         const uint32_t cw = f2::kCoef[2 * kind + xi] ^ (neg ? 0x666666u : 0u);
-        uint32_t P[24];
-        if (mask & 1u) {
-            f2::prod24(P, A0, B0);
-            acc_pair(accO, accX, P, (cw >> c0) & 3u, (cw >> c1) & 3u);
-        }
-        if (mask & 2u) {
-            f2::prod24(P, A1, B1);
-            acc_pair(accO, accX, P, (cw >> (c0 + 4)) & 3u, (cw >> (c1 + 4)) & 3u);
-        }
-        if (kind == f2::kKara && (mask & 4u)) {
-            f2::add12(A0, A0, A1);
-            f2::add12(B0, B0, B1);
-            f2::prod24(P, A0, B0);
-            acc_pair(accO, accX, P, (cw >> (c0 + 8)) & 3u, (cw >> (c1 + 8)) & 3u);
+        // every operand is read from shared memory when its product runs, so
+        // one product call site serves every kind and nothing stays live
+        // beside the accumulators between products
+        const uint32_t np = kind == f2::kKara ? 3u : 2u;
+#pragma unroll 1
+        for (uint32_t j = 0; j < np; ++j) {
+            if (!((mask >> j) & 1u)) continue;
+            uint32_t U[12], V[12], P[24];
+            if (kind == f2::kSqr) {          // U = x0 + x1, 2 x0
+                load_fp(U, sm, xs, 0);
+                if (j == 0) {
+                    uint32_t T[12];
+                    load_fp(T, sm, xs, 1);
+                    f2::add12(U, U, T);
+                } else {
+                    f2::dbl12(U);
+                }
+            } else if (kind == f2::kKara && xi) {   // xi X = (x0 - x1 + 3p, x0 + x1); sum 2 x0 + 3p
+                load_fp(U, sm, xs, 0);
+                if (j == 2) {
+                    const uint32_t z[12] = {0};
+                    f2::dbl12(U);
+                    f2::add3p_sub(U, U, z);
+                } else {
+                    uint32_t T[12];
+                    load_fp(T, sm, xs, 1);
+                    if (j == 0) f2::add3p_sub(U, U, T);
+                    else f2::add12(U, U, T);
+                }
+            } else {                         // x0, x1 (KARA: sum x0 + x1)
+                load_fp(U, sm, xs, j & 1u);
+                if (j == 2) {
+                    uint32_t T[12];
+                    load_fp(T, sm, xs, 1);
+                    f2::add12(U, U, T);
+                }
+            }
+            if (kind == f2::kKara) {        // V = y0, y1, y0 + y1 (doubled when dbl)
+                load_fp(V, sm, ys, j & 1u);
+                if (j == 2) {
+                    uint32_t T[12];
+                    load_fp(T, sm, ys, 1);
+                    f2::add12(V, V, T);
+                }
+                if (dbl) f2::dbl12(V);
+            } else if (kind == f2::kSqr) {  // V = x0 - x1 + 3p, x1
+                load_fp(V, sm, xs, 1);
+                if (j == 0) {
+                    uint32_t T[12];
+                    load_fp(T, sm, xs, 0);
+                    f2::add3p_sub(V, T, V);
+                }
+            } else if (kind == f2::kFpMul) {
+                load_fp(V, sm, ys, yim);
+            } else {                        // NORM: x_j^2
+                load_fp(V, sm, xs, j);
+            }
+            f2::prod24(P, U, V);
+            acc_pair(accO, accX, P, (cw >> (c0 + 4 * j)) & 3u, (cw >> (c1 + 4 * j)) & 3u);
         }
     }
     uint4* x = reinterpret_cast<uint4*>(xch_out);
