@@ -88,6 +88,38 @@ __device__ __forceinline__ void acc_sub(uint32_t* acc, const uint32_t* p) {
           "r"(p[17]), "r"(p[18]), "r"(p[19]), "r"(p[20]), "r"(p[21]), "r"(p[22]), "r"(p[23]));
 }
 
+// acc[0..25] += p[0..25], modulo 2^832
+__device__ __forceinline__ void add26(uint32_t* acc, const uint32_t* p) {
+    asm("add.cc.u32 %0, %0, %26;\n\t"
+        "addc.cc.u32 %1, %1, %27;\n\t"
+        "addc.cc.u32 %2, %2, %28;\n\t"
+        "addc.cc.u32 %3, %3, %29;\n\t"
+        "addc.cc.u32 %4, %4, %30;\n\t"
+        "addc.cc.u32 %5, %5, %31;\n\t"
+        "addc.cc.u32 %6, %6, %32;\n\t"
+        "addc.cc.u32 %7, %7, %33;\n\t"
+        "addc.cc.u32 %8, %8, %34;\n\t"
+        "addc.cc.u32 %9, %9, %35;\n\t"
+        "addc.cc.u32 %10, %10, %36;\n\t"
+        "addc.cc.u32 %11, %11, %37;\n\t"
+        "addc.cc.u32 %12, %12, %38;\n\t"
+        "addc.cc.u32 %13, %13, %39;\n\t"
+        "addc.cc.u32 %14, %14, %40;\n\t"
+        "addc.cc.u32 %15, %15, %41;\n\t"
+        "addc.cc.u32 %16, %16, %42;\n\t"
+        "addc.cc.u32 %17, %17, %43;\n\t"
+        "addc.cc.u32 %18, %18, %44;\n\t"
+        "addc.cc.u32 %19, %19, %45;\n\t"
+        "addc.cc.u32 %20, %20, %46;\n\t"
+        "addc.cc.u32 %21, %21, %47;\n\t"
+        "addc.cc.u32 %22, %22, %48;\n\t"
+        "addc.cc.u32 %23, %23, %49;\n\t"
+        "addc.cc.u32 %24, %24, %50;\n\t"
+        "addc.u32 %25, %25, %51;"
+        : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3]), "+r"(acc[4]), "+r"(acc[5]), "+r"(acc[6]), "+r"(acc[7]), "+r"(acc[8]), "+r"(acc[9]), "+r"(acc[10]), "+r"(acc[11]), "+r"(acc[12]), "+r"(acc[13]), "+r"(acc[14]), "+r"(acc[15]), "+r"(acc[16]), "+r"(acc[17]), "+r"(acc[18]), "+r"(acc[19]), "+r"(acc[20]), "+r"(acc[21]), "+r"(acc[22]), "+r"(acc[23]), "+r"(acc[24]), "+r"(acc[25])
+        : "r"(p[0]), "r"(p[1]), "r"(p[2]), "r"(p[3]), "r"(p[4]), "r"(p[5]), "r"(p[6]), "r"(p[7]), "r"(p[8]), "r"(p[9]), "r"(p[10]), "r"(p[11]), "r"(p[12]), "r"(p[13]), "r"(p[14]), "r"(p[15]), "r"(p[16]), "r"(p[17]), "r"(p[18]), "r"(p[19]), "r"(p[20]), "r"(p[21]), "r"(p[22]), "r"(p[23]), "r"(p[24]), "r"(p[25]));
+}
+
 // acc[0..25] += p (24 limbs), modulo 2^832
 __device__ __forceinline__ void acc_plus(uint32_t* acc, const uint32_t* p) {
     asm("add.cc.u32 %0, %0, %26;\n\t"

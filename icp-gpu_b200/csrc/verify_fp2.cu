@@ -18,7 +18,7 @@
 //   result        canonical Gt compared with 1; optional Miller / Gt outputs
 //
 // Shared memory: 8 block-shared constant slots (0, 1, Frobenius constants),
-// then per pairing 7 groups of 6 Fp2 slots and a 12-slot C area (lines,
+// then per pairing kGroups groups of 6 Fp2 slots and a 12-slot C area (lines,
 // points), then the exchange area (per pairing and coefficient, one 26-word
 // partial sum per half) and per-pairing flags.  An Fp2 slot is 24 words: re
 // then im, each below 2^381 + p.  Every program accumulates, exchanges, meets,
@@ -97,7 +97,7 @@ __device__ __forceinline__ void acc_pair(uint32_t* acc0, uint32_t* acc1, const u
 }
 
 // Phase 1 of an output (product modes): this half's products into both
-// accumulators, acc[1 - half] left in the exchange slot for the partner.
+// accumulators, the partner's component (accX) left in the exchange slot.
 __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bases& bs, uint32_t* xch_out,
                                            int half, uint32_t* own) {
     const uint32_t hdr = f2::kDesc[off], bias = f2::kDesc[off + 1];
