@@ -239,13 +239,7 @@ __device__ __forceinline__ void finish(uint32_t off, const uint32_t* sm, const B
         }
         p[24] = xch_in[24];
         p[25] = xch_in[25];
-        uint32_t c = 0;
-#pragma unroll
-        for (int i = 0; i < 26; ++i) {
-            const uint64_t s = (uint64_t)own[i] + p[i] + c;
-            own[i] = (uint32_t)s;
-            c = (uint32_t)(s >> 32);
-        }
+        f2::add26(own, p);
         uint32_t red[13];
         f2::redc26(red, own);
         if (mode == f2::kModeSimple) {
