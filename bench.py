@@ -315,7 +315,7 @@ def run_gpu(args):
         batching = run_batching(G, WL, ctx, ids)
         if args.serve_seconds > 0:
             serving = run_serving(G, WL, ctx, args.serve_seconds, slots=args.serve_slots,
-                                  max_batch=args.serve_max_batch)
+                                  max_batch=args.serve_max_batch, mode=args.serve_mode)
 
     result = None
     if rank == 0:
@@ -485,12 +485,14 @@ def run_rlc(G, WL, ctx, wl4096, pk_ids4096, n=65536, reps=3):
             "fallback_4096_ms": round(t_fb * 1e3, 2), "per_item_4096_ms": round(t_fb_item * 1e3, 2)}
 
 
-def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192):
+def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ring", ring_blocks_per_sm=0):
     """Serving workload: seeded Poisson stream of requests (sizes log-uniform in
     [1, 512]) over a pool of 40 resident keys, through the continuous-batching
-    server (bls_server_*) under a 4 GiB device-memory cap.  The arrival rate is
-    `load` x the server's measured saturated throughput; latency is submit to
-    completion on the library's steady clock."""
+    server (bls_server_*) under a 4 GiB device-memory cap: `mode` "ring" (one
+    persistent kernel claiming items from a device ring as they are published)
+    or "slots" (`slots` launches of up to `max_batch` items in flight).  The
+    arrival rate is `load` x the server's measured saturated throughput;
+    latency is submit to completion on the library's steady clock."""
     import threading
     pool = WL.config_pool(8192, N_KEYS, seed=5)
     ids = np.array([ctx.register_pk_affine(q) for q in pool["pk_affine"]], dtype=np.int32)
@@ -505,7 +507,12 @@ def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192):
                         np.ascontiguousarray(pk_ids[ix])))
         return out
 
-    with G.Server(ctx, slots=slots, max_batch_items=max_batch, mem_cap_bytes=4 << 30) as srv:
+    if mode == "ring":
+        server = G.Server(ctx, max_batch_items=512, mem_cap_bytes=4 << 30, mode=G.SERVE_RING,
+                          ring_blocks_per_sm=ring_blocks_per_sm)
+    else:
+        server = G.Server(ctx, slots=slots, max_batch_items=max_batch, mem_cap_bytes=4 << 30)
+    with server as srv:
         # saturated throughput: a backlog of requests submitted at once
         _, sizes, starts = WL.poisson_stream(1.0, 4000.0, max_size=512, pool_size=npool, seed=7)
         burst = materialise(starts, sizes)
@@ -559,6 +566,8 @@ def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192):
         "p999_ms": round(float(np.percentile(lat, 99.9)), 3), "max_ms": round(float(lat.max()), 3),
         "launches": int(stats1["launches"] - stats0["launches"]),
         "mem_cap_bytes": 4 << 30, "sizes": "log-uniform [1, 512]", "bit_exact": True,
+        "mode": ("ring: one persistent kernel claiming items five at a time from a device ring"
+                 if mode == "ring" else "slots: %d launches of up to %d items in flight" % (slots, max_batch)),
     }
 
 
@@ -575,8 +584,9 @@ def main():
                     help="comma-separated key counts ingested compressed on the GPU (0 = skip)")
     ap.add_argument("--rlc-items", type=int, default=65536, help="random-linear-combination batch draw (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the serving stream (0 = skip)")
-    ap.add_argument("--serve-slots", type=int, default=6, help="serving: launches in flight")
-    ap.add_argument("--serve-max-batch", type=int, default=1480, help="serving: items per launch")
+    ap.add_argument("--serve-mode", choices=["ring", "slots"], default="slots", help="serving: server mode")
+    ap.add_argument("--serve-slots", type=int, default=8, help="serving: launches in flight")
+    ap.add_argument("--serve-max-batch", type=int, default=740, help="serving: items per launch")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -29,6 +29,19 @@ struct VerifyArgs {
     const uint64_t* pk_norm;
     const uint64_t* g2_corr;
     const uint64_t* pk_corr;
+    // Ring serving (Fp2-lane kernel only): sigs / nhms / pk_index / results are
+    // rings of serve_cap slots (a multiple of 5) in device memory, filled by the
+    // host's copies; the host publishes whole groups of 5 by raising
+    // *serve_avail (items since the start, device memory, written by a copy
+    // after the items' own copies); blocks claim published groups from
+    // *serve_claimed and leave after serve_idle_ns without a claimable group,
+    // when *serve_stop is set, or serve_max_ns after the launch.
+    const volatile uint32_t* serve_avail;
+    const volatile uint32_t* serve_stop;
+    uint32_t* serve_claimed;
+    uint32_t serve_cap;
+    uint64_t serve_idle_ns;
+    uint64_t serve_max_ns;
 };
 
 cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s);
@@ -70,6 +83,7 @@ cudaError_t launch_lines_normalize(const uint64_t* raw, int n, uint64_t* norm, u
 // per-Fp programs (verify_vm.cu).
 cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int blocks_per_sm,
                                 int sms, cudaStream_t s);
+cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks_per_sm, int sms, cudaStream_t s);
 cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, int blocks_per_sm, int sms,
                               cudaStream_t s);
 size_t verify_fp2_smem_bytes();
@@ -89,6 +103,19 @@ struct CtxView {
     const uint64_t* pk_norm;
     const uint64_t* g2_corr;
     const uint64_t* pk_corr;
+    // Ring serving (Fp2-lane kernel only): sigs / nhms / pk_index / results are
+    // rings of serve_cap slots (a multiple of 5) in device memory, filled by the
+    // host's copies; the host publishes whole groups of 5 by raising
+    // *serve_avail (items since the start, device memory, written by a copy
+    // after the items' own copies); blocks claim published groups from
+    // *serve_claimed and leave after serve_idle_ns without a claimable group,
+    // when *serve_stop is set, or serve_max_ns after the launch.
+    const volatile uint32_t* serve_avail;
+    const volatile uint32_t* serve_stop;
+    uint32_t* serve_claimed;
+    uint32_t serve_cap;
+    uint64_t serve_idle_ns;
+    uint64_t serve_max_ns;
 };
 
 }  // namespace bls

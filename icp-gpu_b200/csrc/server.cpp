@@ -18,8 +18,21 @@
 // counted against mem_cap_bytes at creation; the number of slots is reduced
 // to what the budget admits.  Waits are bounded (timeouts), the dispatcher
 // never spins on the device: it sleeps on a condition variable between polls.
+//
+// Ring mode (BLS_SERVE_RING): requests are padded to whole groups of five
+// with identity items and written into host mirrors of a device ring of item
+// slots; one copy stream moves each new range (inputs and sentinel results) to
+// the device and then raises the published-item count in device memory.  One
+// persistent launch of the six-lane kernel claims published groups from a
+// device counter as blocks free up and writes each result into the ring.  The
+// dispatcher copies the results of the in-flight range back, sees a request
+// complete when none of its result slots holds the sentinel any more, copies
+// its results out and frees ring space in order.  Admission is by ring space.
+// The kernel leaves when idle for 20 ms, on destroy, or 60 s after its launch;
+// the dispatcher relaunches it while work is left.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -65,8 +78,32 @@ struct Slot {
 
 }  // namespace
 
+// ring mode state: device ring and its host mirrors (same slot indexing)
+struct Ring {
+    uint32_t cap = 0;                      // item slots, a multiple of 5
+    uint64_t *h_sigs = nullptr, *h_nhms = nullptr;   // pinned mirrors: cap x 12
+    int32_t *h_ids = nullptr, *h_res = nullptr;      // cap
+    uint32_t* h_ctl = nullptr;             // pinned: [0] published items, [1] stop
+    uint64_t *d_sigs = nullptr, *d_nhms = nullptr;
+    int32_t *d_ids = nullptr, *d_res = nullptr;
+    uint32_t* d_ctl = nullptr;             // device: [0] published, [1] stop, [2] claimed
+    cudaStream_t copy = nullptr, kern = nullptr;
+    cudaEvent_t done = nullptr;
+    bool launched = false;
+    uint32_t pub = 0, tail = 0;            // items published / released (monotonic)
+    struct Flight {
+        Pending req;
+        uint32_t start, span;
+        bool complete;
+    };
+    std::deque<Flight> flights;
+};
+constexpr int32_t kSentinel = 0x7fffffff;
+constexpr uint32_t kGroup = 5;
+
 struct bls_server {
     bls_ctx* ctx = nullptr;
+    Ring ring;
     bls_server_config cfg{};
     bls::CtxView view{};
     std::vector<Slot> slots;
@@ -141,11 +178,167 @@ struct bls_server {
         s.busy = false;
     }
 
+    // ---- ring mode
+    int ring_launch() {
+        bls::VerifyArgs a{};
+        a.sigs = ring.d_sigs;
+        a.nhms = ring.d_nhms;
+        a.g2 = view.g2;
+        a.pk_tables = view.pk_tables;
+        a.g2_norm = view.g2_norm;
+        a.pk_norm = view.pk_norm;
+        a.g2_corr = view.g2_corr;
+        a.pk_corr = view.pk_corr;
+        a.pk_index = ring.d_ids;
+        a.pk_identity = view.pk_identity;
+        a.n = 1;
+        a.results = ring.d_res;
+        a.serve_avail = ring.d_ctl;
+        a.serve_stop = ring.d_ctl + 1;
+        a.serve_claimed = ring.d_ctl + 2;
+        a.serve_cap = ring.cap;
+        a.serve_idle_ns = 20ull * 1000 * 1000;
+        a.serve_max_ns = 60ull * 1000 * 1000 * 1000;
+        if (bls::launch_verify_fp2_serve(a, cfg.ring_blocks_per_sm, view.sms, ring.kern) ||
+            cudaEventRecord(ring.done, ring.kern))
+            return BLS_ERR_CUDA;
+        ring.launched = true;
+        ++launches;
+        return BLS_OK;
+    }
+
+    // host mirror range [a, a + n) (ring positions, may wrap) to the device
+    template <typename T>
+    int ring_copy_in(T* dst, const T* src, size_t per, uint32_t a, uint32_t n) {
+        const uint32_t s0 = a % ring.cap, first = std::min(n, ring.cap - s0);
+        if (cudaMemcpyAsync(dst + per * s0, src + per * s0, sizeof(T) * per * first, cudaMemcpyHostToDevice,
+                            ring.copy))
+            return BLS_ERR_CUDA;
+        if (first < n && cudaMemcpyAsync(dst, src, sizeof(T) * per * (n - first), cudaMemcpyHostToDevice, ring.copy))
+            return BLS_ERR_CUDA;
+        return BLS_OK;
+    }
+
+    // one pass: results of the in-flight range, completions, admissions and
+    // their publication, (re)launch; `progressed` when anything moved
+    int ring_step(bool& progressed) {
+        const uint32_t inflight = ring.pub - ring.tail;
+        if (inflight) {
+            const uint32_t s0 = ring.tail % ring.cap, first = std::min(inflight, ring.cap - s0);
+            if (cudaMemcpyAsync(ring.h_res + s0, ring.d_res + s0, 4 * (size_t)first, cudaMemcpyDeviceToHost,
+                                ring.copy) ||
+                (first < inflight && cudaMemcpyAsync(ring.h_res, ring.d_res, 4 * (size_t)(inflight - first),
+                                                     cudaMemcpyDeviceToHost, ring.copy)) ||
+                cudaStreamSynchronize(ring.copy))
+                return BLS_ERR_CUDA;
+        }
+        const int64_t t = now_ns();
+        bool any_done = false;
+        for (auto& f : ring.flights) {
+            if (f.complete) continue;
+            bool all = true;
+            for (uint32_t k = f.span; k-- > 0;)
+                if (ring.h_res[(f.start + k) % ring.cap] == kSentinel) {
+                    all = false;
+                    break;
+                }
+            if (!all) continue;
+            for (int k = 0; k < f.req.n; ++k) f.req.results[k] = ring.h_res[(f.start + k) % ring.cap];
+            done[f.req.ticket] = t;
+            items += f.req.n;
+            f.complete = true;
+            any_done = true;
+        }
+        while (!ring.flights.empty() && ring.flights.front().complete) {
+            ring.tail += ring.flights.front().span;
+            ring.flights.pop_front();
+        }
+        if (any_done) {
+            cv_done.notify_all();
+            progressed = true;
+        }
+        const uint32_t from = ring.pub;
+        while (!queue.empty()) {
+            Pending& q = queue.front();
+            const uint32_t span = ((uint32_t)q.n + kGroup - 1) / kGroup * kGroup;
+            if (ring.pub - ring.tail + span > ring.cap) break;
+            for (uint32_t k = 0; k < span; ++k) {
+                const uint32_t slot = (ring.pub + k) % ring.cap;
+                ring.h_res[slot] = kSentinel;
+                if (k < (uint32_t)q.n) {
+                    memcpy(ring.h_sigs + 12 * (size_t)slot, q.sigs.data() + 96 * (size_t)k, 96);
+                    memcpy(ring.h_nhms + 12 * (size_t)slot, q.nhms.data() + 12 * (size_t)k, 96);
+                    ring.h_ids[slot] = q.ids[k];
+                } else {  // padding: identity points, key 0 (both pairs skipped)
+                    memset(ring.h_sigs + 12 * (size_t)slot, 0, 96);
+                    memset(ring.h_nhms + 12 * (size_t)slot, 0, 96);
+                    ring.h_ids[slot] = 0;
+                }
+            }
+            if ((uint64_t)q.n > max_batch) max_batch = q.n;
+            ring.flights.push_back(Ring::Flight{std::move(q), ring.pub, span, false});
+            ring.pub += span;
+            queue.pop_front();
+        }
+        if (ring.pub != from) {
+            const uint32_t n = ring.pub - from;
+            int rc;
+            if ((rc = ring_copy_in(ring.d_sigs, ring.h_sigs, 12, from, n)) ||
+                (rc = ring_copy_in(ring.d_nhms, ring.h_nhms, 12, from, n)) ||
+                (rc = ring_copy_in(ring.d_ids, ring.h_ids, 1, from, n)) ||
+                (rc = ring_copy_in(ring.d_res, ring.h_res, 1, from, n)))
+                return rc;
+            // the count goes up only after the items' copies (same stream)
+            ring.h_ctl[0] = ring.pub;
+            if (cudaMemcpyAsync(ring.d_ctl, ring.h_ctl, 4, cudaMemcpyHostToDevice, ring.copy) ||
+                cudaStreamSynchronize(ring.copy))
+                return BLS_ERR_CUDA;
+            progressed = true;
+        }
+        bool pending = false;
+        for (auto& f : ring.flights) pending = pending || !f.complete;
+        if (pending && !(ring.launched && cudaEventQuery(ring.done) == cudaErrorNotReady)) {
+            int rc = ring_launch();
+            if (rc) return rc;
+            progressed = true;
+        }
+        return BLS_OK;
+    }
+
+    void run_ring() {
+        std::unique_lock<std::mutex> lk(mu);
+        while (true) {
+            bool progressed = false;
+            int rc = ring_step(progressed);
+            if (rc) {
+                error = rc;
+                cv_done.notify_all();
+                return;
+            }
+            if (stop && queue.empty() && ring.flights.empty()) break;
+            if (!progressed) cv_work.wait_for(lk, std::chrono::microseconds(ring.flights.empty() ? 2000 : 20));
+        }
+        lk.unlock();
+        ring_stop();
+    }
+
+    void ring_stop() {
+        if (!ring.h_ctl || !ring.d_ctl) return;
+        ring.h_ctl[1] = 1;
+        cudaMemcpyAsync(ring.d_ctl + 1, ring.h_ctl + 1, 4, cudaMemcpyHostToDevice, ring.copy);
+        cudaStreamSynchronize(ring.copy);
+        if (ring.kern) cudaStreamSynchronize(ring.kern);
+    }
+
     void run() {
         if (cudaSetDevice(view.device) != cudaSuccess) {
             std::lock_guard<std::mutex> lk(mu);
             error = BLS_ERR_CUDA;
             cv_done.notify_all();
+            return;
+        }
+        if (cfg.mode == BLS_SERVE_RING) {
+            run_ring();
             return;
         }
         std::unique_lock<std::mutex> lk(mu);
@@ -194,7 +387,10 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
     if (s->cfg.slots <= 0) s->cfg.slots = 3;
     if (s->cfg.max_batch_items <= 0) s->cfg.max_batch_items = 16384;
     if (s->cfg.mem_cap_bytes == 0) s->cfg.mem_cap_bytes = (size_t)4 << 30;
-    if (s->cfg.sig_format != BLS_SIG_AFFINE && s->cfg.sig_format != BLS_SIG_COMPRESSED) {
+    if ((s->cfg.sig_format != BLS_SIG_AFFINE && s->cfg.sig_format != BLS_SIG_COMPRESSED) ||
+        (s->cfg.mode != BLS_SERVE_SLOTS && s->cfg.mode != BLS_SERVE_RING) ||
+        (s->cfg.mode == BLS_SERVE_RING && s->cfg.sig_format != BLS_SIG_AFFINE) || s->cfg.ring_items < 0 ||
+        s->cfg.ring_blocks_per_sm < 0) {
         delete s;
         return BLS_ERR_INVALID;
     }
@@ -202,6 +398,48 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
     if (cudaSetDevice(s->view.device) != cudaSuccess) {
         delete s;
         return BLS_ERR_CUDA;
+    }
+    if (s->cfg.mode == BLS_SERVE_RING) {
+        if (s->view.lanes != 6 && s->view.lanes != 0) {  // the ring is served by the six-lane kernel
+            delete s;
+            return BLS_ERR_INVALID;
+        }
+        Ring& r = s->ring;
+        if (s->cfg.ring_blocks_per_sm == 0) s->cfg.ring_blocks_per_sm = 4;
+        const int most = bls::verify_lanes_blocks_per_sm(6);
+        if (most > 0 && s->cfg.ring_blocks_per_sm > most) s->cfg.ring_blocks_per_sm = most;
+        uint64_t cap = s->cfg.ring_items > 0 ? (uint64_t)s->cfg.ring_items : 65535u;
+        const uint64_t least = (uint64_t)s->cfg.max_batch_items + 2 * kGroup;
+        if (cap < least) cap = least;
+        cap = (cap + kGroup - 1) / kGroup * kGroup;
+        if (cap * 200 + 64 > s->cfg.mem_cap_bytes || cap > (1u << 30)) {
+            delete s;
+            return BLS_ERR_NOMEM;
+        }
+        r.cap = (uint32_t)cap;
+        bool ok = cudaHostAlloc((void**)&r.h_sigs, cap * 96, 0) == cudaSuccess &&
+                  cudaHostAlloc((void**)&r.h_nhms, cap * 96, 0) == cudaSuccess &&
+                  cudaHostAlloc((void**)&r.h_ids, cap * 4, 0) == cudaSuccess &&
+                  cudaHostAlloc((void**)&r.h_res, cap * 4, 0) == cudaSuccess &&
+                  cudaHostAlloc((void**)&r.h_ctl, 64, 0) == cudaSuccess &&
+                  cudaMalloc((void**)&r.d_sigs, cap * 96) == cudaSuccess &&
+                  cudaMalloc((void**)&r.d_nhms, cap * 96) == cudaSuccess &&
+                  cudaMalloc((void**)&r.d_ids, cap * 4) == cudaSuccess &&
+                  cudaMalloc((void**)&r.d_res, cap * 4) == cudaSuccess &&
+                  cudaMalloc((void**)&r.d_ctl, 64) == cudaSuccess && cudaMemset(r.d_ctl, 0, 64) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&r.copy, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&r.kern, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaDeviceSynchronize() == cudaSuccess;
+        if (ok) memset(r.h_ctl, 0, 64);
+        if (!ok) {
+            bls_server_destroy(s);
+            return BLS_ERR_NOMEM;
+        }
+        bls::verify_lanes_blocks_per_sm(6);
+        s->worker = std::thread([s] { s->run(); });
+        *out = s;
+        return BLS_OK;
     }
     size_t m = (size_t)s->cfg.max_batch_items;
     size_t per_slot = m * (s->sig_bytes() + 96 + 4 + 4 + 96 + 4) + 256;
@@ -244,6 +482,17 @@ void bls_server_destroy(bls_server* s) {
         s->worker.join();
     }
     cudaSetDevice(s->view.device);
+    {
+        Ring& r = s->ring;
+        s->ring_stop();
+        for (void* p : {(void*)r.h_sigs, (void*)r.h_nhms, (void*)r.h_ids, (void*)r.h_res, (void*)r.h_ctl})
+            if (p) cudaFreeHost(p);
+        for (void* p : {(void*)r.d_sigs, (void*)r.d_nhms, (void*)r.d_ids, (void*)r.d_res, (void*)r.d_ctl})
+            if (p) cudaFree(p);
+        if (r.done) cudaEventDestroy(r.done);
+        if (r.copy) cudaStreamDestroy(r.copy);
+        if (r.kern) cudaStreamDestroy(r.kern);
+    }
     for (auto& sl : s->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         for (void* p : {sl.h_sigs, sl.h_nhms, sl.h_ids, sl.h_res})

@@ -341,6 +341,47 @@ __device__ __forceinline__ bool emit_group(const Ctx& c, int g, uint64_t* out) {
     return one;
 }
 
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Ring serving, thread 0 of a block: claim the next published group of five
+// items (all in device memory).  False when the block should leave: the stop
+// flag, serve_idle_ns without a claimable group, or serve_max_ns after the
+// launch; the loop also has an iteration cap, so every wait ends.
+__device__ bool serve_claim(const VerifyArgs& a, uint64_t t_launch, uint32_t* base) {
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        const uint32_t cur = *reinterpret_cast<volatile uint32_t*>(a.serve_claimed);
+        const uint32_t av = *a.serve_avail;
+        if ((int32_t)(av - cur) > 0) {
+            if (atomicCAS(a.serve_claimed, cur, cur + kPairsPerBlock) == cur) {
+                *base = cur;
+                return true;
+            }
+            continue;
+        }
+        const uint64_t now = globaltimer_ns();
+        if (*a.serve_stop || now - t0 > a.serve_idle_ns || now - t_launch > a.serve_max_ns) return false;
+        __nanosleep(500);
+    }
+    return false;
+}
+
+// 6 x u64 read at L2 (not L1): a serving ring rewrites its slots by copies
+__device__ __forceinline__ fp fp_load_u64_cg(const uint64_t* v) {
+    fp r;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const unsigned long long x = __ldcg(reinterpret_cast<const unsigned long long*>(v) + i);
+        r.w[2 * i] = (uint32_t)x;
+        r.w[2 * i + 1] = (uint32_t)(x >> 32);
+    }
+    return r;
+}
+
 __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const uint32_t* __restrict__ in_status) {
     extern __shared__ uint4 smem4[];
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem4);
@@ -364,9 +405,23 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
 
     int next = blockIdx.x * kPairsPerBlock;
     const int stride = gridDim.x * kPairsPerBlock;
+    const bool serving = a.serve_avail != nullptr;
+    const uint64_t t_launch = serving ? globaltimer_ns() : 0;
     for (;;) {
         int base;
-        if (a.work_counter) {
+        if (serving) {
+            if (threadIdx.x == 0) {
+                uint32_t b = 0;
+                const bool go = serve_claim(a, t_launch, &b);
+                bcast[0] = b % a.serve_cap;
+                bcast[1] = go ? 1u : 0u;
+            }
+            __syncthreads();
+            base = (int)bcast[0];
+            const bool go = bcast[1] != 0;
+            __syncthreads();
+            if (!go) break;
+        } else if (a.work_counter) {
             if (threadIdx.x == 0) bcast[0] = (uint32_t)atomicAdd(a.work_counter, kPairsPerBlock);
             __syncthreads();
             base = (int)bcast[0];
@@ -375,9 +430,9 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
             base = next;
             next += stride;
         }
-        if (base >= a.n) break;
+        if (!serving && base >= a.n) break;
         const int item = base + (c.active ? pi : 0);
-        const bool have = c.active && item < a.n;
+        const bool have = c.active && (serving || item < a.n);
         bool skip1 = true, skip2 = true;
         const uint64_t* pk = g2_lines;
         const uint64_t* pk_cf = a.g2_corr;
@@ -386,9 +441,9 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
             const uint64_t* s = a.sig_xy ? a.sig_xy + 12 * (size_t)item : (const uint64_t*)a.sigs + 12 * (size_t)item;
             const uint64_t* h = a.nhms + 12 * (size_t)item;
             if (in_status) status = (int32_t)in_status[item];
-            fp sx = fp_load_u64(s), sy = fp_load_u64(s + 6);
-            fp hx = fp_load_u64(h), hy = fp_load_u64(h + 6);
-            int64_t pki = a.pk_index ? (int64_t)a.pk_index[item] : (int64_t)item;
+            fp sx = fp_load_u64_cg(s), sy = fp_load_u64_cg(s + 6);
+            fp hx = fp_load_u64_cg(h), hy = fp_load_u64_cg(h + 6);
+            int64_t pki = a.pk_index ? (int64_t)__ldcg(a.pk_index + item) : (int64_t)item;
             pk = (norm ? a.pk_norm : a.pk_tables) + kCoeffU64 * pki;
             if (norm) pk_cf = a.pk_corr + 12 * pki;
             skip1 = g1_limbs_identity(sx, sy) || status != 0;
@@ -467,6 +522,18 @@ int resident() {
 size_t verify_fp2_smem_bytes() { return smem_bytes(); }
 
 int verify_fp2_blocks_per_sm() { return resident(); }
+
+// ring serving: one persistent block per resident slot
+cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks_per_sm, int sms, cudaStream_t s) {
+    if (!a.serve_avail || !a.serve_stop || !a.serve_claimed || a.serve_cap == 0 || a.serve_cap % kPairsPerBlock)
+        return cudaErrorInvalidValue;
+    cudaError_t e = configure();
+    if (e != cudaSuccess) return e;
+    const int res = resident();
+    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm : (res > 0 ? res : 1);
+    k_verify_fp2<<<per_sm * sms, kThreads, smem_bytes(), s>>>(a, nullptr);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, int blocks_per_sm, int sms,
                               cudaStream_t s) {

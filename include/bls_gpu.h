@@ -217,9 +217,25 @@ typedef struct bls_server bls_server;
 typedef struct {
     int sig_format;            /* of every request submitted */
     int slots;                 /* launches in flight (0 = 3) */
-    int max_batch_items;       /* items per launch (0 = 16384) */
-    size_t mem_cap_bytes;      /* device memory for the slots (0 = 4 GiB) */
+    int max_batch_items;       /* items per launch / largest request (0 = 16384) */
+    size_t mem_cap_bytes;      /* device memory for the slots or the ring (0 = 4 GiB) */
+    int mode;                  /* BLS_SERVE_SLOTS (0) or BLS_SERVE_RING */
+    int ring_items;            /* ring mode: ring slots, rounded up to a multiple of 5 (0 = 65535) */
+    int ring_blocks_per_sm;    /* ring mode: resident blocks of the kernel per SM (0 = 4); fewer
+                                  verifications share an SM, so each finishes sooner */
 } bls_server_config;
+
+/* Serving modes.  SLOTS: the launch slots above.  RING (affine signatures,
+ * six-lane kernel): one persistent verify kernel claims items five at a time
+ * from a ring in device memory as the dispatcher publishes them, so a request
+ * starts as soon as a block is free instead of waiting for a launch slot.  The
+ * dispatcher copies requests in, publishes them with one more small copy and
+ * polls the results back.  The kernel leaves after 20 ms without work (the
+ * next request relaunches it), when the server is destroyed, or 60 s after
+ * its launch; every wait in it is bounded.  Admission is by ring space
+ * (ring_items x 200 bytes, counted against mem_cap_bytes). */
+#define BLS_SERVE_SLOTS 0
+#define BLS_SERVE_RING 1
 
 int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** out);
 /* waits for in-flight work, then frees the server */

@@ -97,3 +97,62 @@ def test_admission_and_argument_errors(pool):
             assert (res == pool["expect"][:5]).all()
             with pytest.raises(G.GpuError):   # unknown ticket: times out
                 srv.wait(t + 1000, timeout_ms=10)
+
+
+def _submit_all(srv, pool, pk_ids, reqs, threads=3):
+    tickets = [None] * len(reqs)
+
+    def submit(k0):
+        for k in range(k0, len(reqs), threads):
+            ix = reqs[k]
+            tickets[k] = srv.submit(pool["sigs"][ix], pool["nhms"][ix], pk_ids[ix])
+
+    th = [threading.Thread(target=submit, args=(k,)) for k in range(threads)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    return tickets
+
+
+def test_ring_mode_equals_alone(pool):
+    """Ring mode: one persistent kernel takes items as they are published; every
+    request's results equal verifying it alone, for sizes from 1 upwards and a
+    ring smaller than the stream (admission waits for ring space)."""
+    with G.Context() as ctx:
+        ids = _ids(ctx, pool)
+        pk_ids = ids[pool["pk_index"]]
+        reqs = _requests(pool, 80, 300, seed=3) + [np.array([7]), np.array([8, 9])]
+        alone = [ctx.verify(pool["sigs"][ix], pool["nhms"][ix], pk_ids[ix]) for ix in reqs]
+        with G.Server(ctx, max_batch_items=512, mode=G.SERVE_RING, ring_items=1000) as srv:
+            tickets = _submit_all(srv, pool, pk_ids, reqs)
+            for k, (ticket, t_sub, res) in enumerate(tickets):
+                t_done = srv.wait(ticket, timeout_ms=60000)
+                assert t_done >= t_sub
+                assert (res == alone[k]).all()
+                assert (res == pool["expect"][reqs[k]]).all()
+            st = srv.stats()
+        assert st["items"] == sum(len(ix) for ix in reqs)
+        assert st["launches"] >= 1
+
+
+def test_ring_mode_idle_relaunch(pool):
+    """The ring kernel leaves after 20 ms without work; a later request relaunches it."""
+    import time
+    with G.Context() as ctx:
+        ids = _ids(ctx, pool)
+        pk_ids = ids[pool["pk_index"]]
+        with G.Server(ctx, max_batch_items=64, mode=G.SERVE_RING) as srv:
+            for a in (0, 30, 60):
+                t, _, res = srv.submit(pool["sigs"][a:a + 17], pool["nhms"][a:a + 17], pk_ids[a:a + 17])
+                srv.wait(t, timeout_ms=60000)
+                assert (res == pool["expect"][a:a + 17]).all()
+                time.sleep(0.1)
+            st = srv.stats()
+        assert st["launches"] == 3
+
+
+def test_ring_mode_rejects_compressed():
+    with G.Context() as ctx:
+        with pytest.raises(G.GpuError):
+            G.Server(ctx, compressed=True, mode=G.SERVE_RING)
