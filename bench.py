@@ -306,6 +306,7 @@ def run_gpu(args):
     e2e_s = max_over_ranks(pg, sum(e2e_times), dev)
     e2e_value = whole_job_rate(N_ITEMS, world, args.steps, e2e_s)
 
+    chain_timad = ctx.imad_chain_rate() / 1e12
     batching = serving = ingest = hashing = rlc = None
     if not args.no_extras:
         sizes = [int(v) for v in args.ingest_keys.split(",") if int(v) > 0]
@@ -332,6 +333,10 @@ def run_gpu(args):
             "kernel": ("k_verify_fp2" if args.lanes == 6 else "k_verify_lanes<%d>" % args.lanes) if args.lanes > 1
             else "k_verify",
             "kernel_ms": round(kernel_ms, 4),
+            "chain_ceiling": round(chain_timad, 3),
+            "frac_of_chain_ceiling": round(achieved_timad / chain_timad, 4),
+            "chain_ceiling_basis": "measured: 12 x 12-limb carry-chain products (288 IMAD each) in a loop with the "
+                                   "verify kernel's block shape and occupancy (bls_imad_chain_rate)",
         }
         result = {
             "metric": METRIC, "value": round(value, 1), "unit": "verifies/s", "n_gpus": world,

@@ -112,6 +112,7 @@ def lib():
         L.bls_ctx_stream.restype = P
         L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
         L.bls_neg_hash_to_g1.argtypes = [P, P, P, I, P, I, P]
+        L.bls_imad_chain_rate.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.bls_verify_batch_rlc.argtypes = [P, ctypes.POINTER(Batch), P, P, ctypes.POINTER(I), P]
         L.bls_verify_messages.argtypes = [P, I, P, P, P, P, I, P, I, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
@@ -378,6 +379,12 @@ class Context:
                                                  _ptr(buf), _ptr(off), _ptr(ids), n, _ptr(d) if d.size else None,
                                                  d.size, _ptr(res)), "bls_verify_messages")
         return res
+
+    def imad_chain_rate(self):
+        """IMAD-pipe instructions/s of the carry-chain product loop (bls_imad_chain_rate)."""
+        v = ctypes.c_double(0.0)
+        self._check(self.lib.bls_imad_chain_rate(self.h, ctypes.byref(v)), "bls_imad_chain_rate")
+        return v.value
 
     def g1_decompress(self, compressed):
         src = np.ascontiguousarray(np.frombuffer(bytes(compressed), dtype=np.uint8))

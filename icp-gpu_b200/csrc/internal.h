@@ -88,6 +88,7 @@ cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, in
                               cudaStream_t s);
 size_t verify_fp2_smem_bytes();
 int verify_fp2_blocks_per_sm();
+cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s, double* imad_per_s);
 size_t verify_lanes_smem_bytes(int lanes);
 // blocks of the lane-parallel kernel resident per SM (occupancy calculator)
 int verify_lanes_blocks_per_sm(int lanes);

@@ -503,6 +503,32 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
 
 size_t smem_bytes() { return (size_t)(kSlotArea + kXchArea + kFlagArea) * 4; }
 
+// The carry-chain ceiling the verify kernel is measured against: every thread
+// runs `iters` 12 x 12-limb products (prod24: 144 mul.lo + 144 mul.hi chained
+// through the carry flag, 288 IMAD-pipe instructions) and adds each into a
+// 26-limb accumulator, with the verify kernel's block shape and occupancy and
+// no loads, barriers or reductions; one operand changes every iteration so
+// no product can be hoisted.
+__global__ void __launch_bounds__(kThreads, 6) k_imad_chain(int iters, uint32_t* out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t U[12], V[12], acc[26] = {0}, P[24];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        U[i] = 0x9e3779b9u * (t + i) + 0x7f4a7c15u;
+        V[i] = 0x85ebca6bu * (t ^ (i << 8)) + 0xc2b2ae35u;
+    }
+#pragma unroll 1
+    for (int k = 0; k < iters; ++k) {
+        f2::prod24(P, U, V);
+        f2::acc_plus(acc, P);
+        V[0] += 1u;
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int i = 0; i < 26; ++i) x ^= acc[i];
+    out[t] = x;
+}
+
 cudaError_t configure() {
     static cudaError_t done =
         cudaFuncSetAttribute(k_verify_fp2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes());
@@ -522,6 +548,32 @@ int resident() {
 size_t verify_fp2_smem_bytes() { return smem_bytes(); }
 
 int verify_fp2_blocks_per_sm() { return resident(); }
+
+// IMAD-pipe instructions per second of the carry-chain product loop on the
+// whole device (blocks: 6 per SM, as the verify kernel runs); `out` must hold
+// 6 x sms x 64 words.  Times one warm launch with events on `s`.
+cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s, double* imad_per_s) {
+    const int blocks = 6 * sms;
+    cudaEvent_t a, b;
+    cudaError_t e;
+    if ((e = cudaEventCreate(&a)) != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&b)) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return e;
+    }
+    k_imad_chain<<<blocks, kThreads, 0, s>>>(iters / 10 + 1, out);   // warm-up
+    cudaEventRecord(a, s);
+    k_imad_chain<<<blocks, kThreads, 0, s>>>(iters, out);
+    cudaEventRecord(b, s);
+    e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e == cudaSuccess) *imad_per_s = (double)blocks * kThreads * iters * 288.0 / (ms * 1e-3);
+    return e;
+}
 
 // ring serving: one persistent block per resident slot
 cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks_per_sm, int sms, cudaStream_t s) {

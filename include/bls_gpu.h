@@ -205,6 +205,12 @@ typedef struct {
 int bls_autotune(bls_ctx* ctx, const bls_batch* sample_device, int repeats, bls_tune_point* points,
                  int max_points, int* n_points);
 
+/* Measured ceiling for the roofline: IMAD-pipe instructions per second of a
+ * loop of 12 x 12-limb carry-chain products (the verify kernel's multiply
+ * form: mul.lo / mul.hi chained through the carry flag) with the verify
+ * kernel's block shape and occupancy, on the whole device. */
+int bls_imad_chain_rate(bls_ctx* ctx, double* imad_per_s);
+
 /* ---- serving: continuous batching of arriving requests ----
  * A server owns a dispatcher thread and `slots` launch slots (each a stream
  * with its own pinned and device buffers).  Submitted requests queue; when a

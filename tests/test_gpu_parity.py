@@ -145,3 +145,13 @@ def test_empty_and_single(ctx, golden):
     assert list(ctx.verify(golden["sig_294_g1"][None], golden["neg_hm_7_g1"][None], [pk])) == [1]
     with pytest.raises(G.GpuError):
         ctx.verify(golden["sig_294_g1"][None], golden["neg_hm_7_g1"][None], [10**6])
+
+
+def test_imad_chain_ceiling_is_plausible():
+    """The measured carry-chain ceiling lies between 1 T and the nominal peak
+    (SMs x 64 IMAD per clock x 2.1 GHz)."""
+    import torch
+    with G.Context() as c:
+        rate = c.imad_chain_rate()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert 1e12 < rate < sms * 64 * 2.1e9
