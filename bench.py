@@ -316,7 +316,8 @@ def run_gpu(args):
         batching = run_batching(G, WL, ctx, ids)
         if args.serve_seconds > 0:
             serving = run_serving(G, WL, ctx, args.serve_seconds, slots=args.serve_slots,
-                                  max_batch=args.serve_max_batch, mode=args.serve_mode)
+                                  max_batch=args.serve_max_batch, mode=args.serve_mode,
+                                  ring_blocks_per_sm=args.serve_ring_blocks)
 
     result = None
     if rank == 0:
@@ -571,8 +572,8 @@ def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ri
         "p999_ms": round(float(np.percentile(lat, 99.9)), 3), "max_ms": round(float(lat.max()), 3),
         "launches": int(stats1["launches"] - stats0["launches"]),
         "mem_cap_bytes": 4 << 30, "sizes": "log-uniform [1, 512]", "bit_exact": True,
-        "mode": ("ring: one persistent kernel claiming items five at a time from a device ring"
-                 if mode == "ring" else "slots: %d launches of up to %d items in flight" % (slots, max_batch)),
+        "mode": ("ring: one persistent kernel (%d blocks per SM) claiming items five at a time from a device "
+                 "ring" % (ring_blocks_per_sm or 4) if mode == "ring" else "slots: %d launches of up to %d items in flight" % (slots, max_batch)),
     }
 
 
@@ -589,7 +590,9 @@ def main():
                     help="comma-separated key counts ingested compressed on the GPU (0 = skip)")
     ap.add_argument("--rlc-items", type=int, default=65536, help="random-linear-combination batch draw (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the serving stream (0 = skip)")
-    ap.add_argument("--serve-mode", choices=["ring", "slots"], default="slots", help="serving: server mode")
+    ap.add_argument("--serve-mode", choices=["ring", "slots"], default="ring", help="serving: server mode")
+    ap.add_argument("--serve-ring-blocks", type=int, default=4,
+                    help="serving, ring mode: resident verify blocks per SM")
     ap.add_argument("--serve-slots", type=int, default=8, help="serving: launches in flight")
     ap.add_argument("--serve-max-batch", type=int, default=740, help="serving: items per launch")
     args = ap.parse_args()

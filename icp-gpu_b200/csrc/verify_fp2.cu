@@ -349,10 +349,13 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 
 // Ring serving, thread 0 of a block: claim the next published group of five
 // items (all in device memory).  False when the block should leave: the stop
-// flag, serve_idle_ns without a claimable group, or serve_max_ns after the
-// launch; the loop also has an iteration cap, so every wait ends.
+// flag, serve_idle_ns in which the published count did not move (idle for the
+// whole kernel, not just for this block: a block that loses claims to others
+// while work keeps arriving stays), or serve_max_ns after the launch; the loop
+// also has an iteration cap, so every wait ends.
 __device__ bool serve_claim(const VerifyArgs& a, uint64_t t_launch, uint32_t* base) {
-    const uint64_t t0 = globaltimer_ns();
+    uint64_t t_moved = globaltimer_ns();
+    uint32_t seen = *a.serve_avail;
     for (uint32_t it = 0; it < (1u << 26); ++it) {
         const uint32_t cur = *reinterpret_cast<volatile uint32_t*>(a.serve_claimed);
         const uint32_t av = *a.serve_avail;
@@ -364,7 +367,11 @@ __device__ bool serve_claim(const VerifyArgs& a, uint64_t t_launch, uint32_t* ba
             continue;
         }
         const uint64_t now = globaltimer_ns();
-        if (*a.serve_stop || now - t0 > a.serve_idle_ns || now - t_launch > a.serve_max_ns) return false;
+        if (av != seen) {
+            seen = av;
+            t_moved = now;
+        }
+        if (*a.serve_stop || now - t_moved > a.serve_idle_ns || now - t_launch > a.serve_max_ns) return false;
         __nanosleep(500);
     }
     return false;
