@@ -59,6 +59,9 @@ IMAD_PER_CLK_PER_SM = 64
 # fraction; work it adds lowers it.
 ALGO_FP_MULS_PER_VERIFY = 16941
 ALGO_IMAD_PER_VERIFY = ALGO_FP_MULS_PER_VERIFY * IMAD_PER_FP_MUL
+# DRAM bytes of one 4,096-verify launch of the verify kernel, measured with ncu
+# (1.71 MB read, 0 written): the kernel is not memory-bound.
+DRAM_BYTES_PER_LAUNCH = 1706752
 
 
 def dist_env():
@@ -326,7 +329,10 @@ def run_gpu(args):
         achieved_timad = ALGO_IMAD_PER_VERIFY * N_ITEMS / (kernel_ms / 1e3) / 1e12
         roofline = {
             "bound": "int32-imad", "achieved": round(achieved_timad, 3), "peak": round(peak_timad, 3),
-            "unit": "TIMAD/s", "frac": round(achieved_timad / peak_timad, 4), "traffic": None,
+            "unit": "TIMAD/s", "frac": round(achieved_timad / peak_timad, 4), "traffic": DRAM_BYTES_PER_LAUNCH,
+            "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-verify launch, ncu "
+                             "capture summarised in profiles/k_verify_fp2_keyset4096.md (line tables and points; "
+                             "the bound is the IMAD pipe, not DRAM)",
             "peak_basis": "%d SMs x 64 IMAD/clk x %.0f MHz (median SM clock sampled during the timed region)"
                           % (sms, clk),
             "algorithmic_imad_per_verify": ALGO_IMAD_PER_VERIFY,
