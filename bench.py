@@ -41,16 +41,14 @@ N_KEYS = 40
 SEED = 2
 METRIC = "BLS12-381 verifies/s, batched vs plain launch, bit-exact; serve p50/p99 ms"
 
-# Fp multiplies per verification in this implementation (icp-gpu_b200/csrc):
-#   Miller loop: 136 line evaluations x 43 (mul_by_014 39 + 2 x fp2_mul_fp 2)
-#                + 62 Fp12 squarings x 36                         = 8,080
-#   final exp:   easy part 861 (inverse 719, 2 Fp12 mul, Frobenius^2)
-#                + 2 cyclotomic squares x 18 + 5 cyc_exp x 1,404
-#                + 10 Fp12 mul x 54 + 6 Frobenius x 17            = 8,559
-# and 588 IMAD-pipe instructions per multiply (12 rows x (48 mad + 1 mul.lo)).
-FP_MULS_PER_VERIFY = 8080 + 8559
-IMAD_PER_FP_MUL = 588
-IMAD_PER_VERIFY = FP_MULS_PER_VERIFY * IMAD_PER_FP_MUL
+# Multiply instructions per verification in this implementation (the
+# six-lane kernel's generated op sequence, counted by gen_fp2ops.py over the
+# 653 programs of one verification): 20,684 products of 12 x 12 limbs, each by
+# one level of limb Karatsuba (three 6 x 6 products: 216 mul.lo / mul.hi), and
+# 7,284 Montgomery reductions (12 rows x 25) = 6,652,944.
+OWN_PRODUCTS_PER_VERIFY = 20684
+OWN_REDC_PER_VERIFY = 7284
+IMAD_PER_VERIFY = OWN_PRODUCTS_PER_VERIFY * 216 + OWN_REDC_PER_VERIFY * 300
 IMAD_PER_CLK_PER_SM = 64
 # Algorithmic work per verification, the fixed roofline numerator: the
 # reference's operation count (gpu-crypto/cuda/api.cu:22-91 over
@@ -58,6 +56,7 @@ IMAD_PER_CLK_PER_SM = 64
 # implementation saves (lazy reduction, a cheaper inverse) raises the achieved
 # fraction; work it adds lowers it.
 ALGO_FP_MULS_PER_VERIFY = 16941
+IMAD_PER_FP_MUL = 588   # the reference CIOS multiply: 12 rows x (24 for a b_i + 1 for m + 24 for m p)
 ALGO_IMAD_PER_VERIFY = ALGO_FP_MULS_PER_VERIFY * IMAD_PER_FP_MUL
 # DRAM bytes of one 4,096-verify launch of the verify kernel, measured with ncu
 # (1.71 MB read, 0 written): the kernel is not memory-bound.
@@ -336,7 +335,8 @@ def run_gpu(args):
             "peak_basis": "%d SMs x 64 IMAD/clk x %.0f MHz (median SM clock sampled during the timed region)"
                           % (sms, clk),
             "algorithmic_imad_per_verify": ALGO_IMAD_PER_VERIFY,
-            "own_imad_per_verify": IMAD_PER_VERIFY, "own_fp_muls_per_verify": FP_MULS_PER_VERIFY,
+            "own_imad_per_verify": IMAD_PER_VERIFY, "own_products_per_verify": OWN_PRODUCTS_PER_VERIFY,
+            "own_reductions_per_verify": OWN_REDC_PER_VERIFY,
             "kernel": ("k_verify_fp2" if args.lanes == 6 else "k_verify_lanes<%d>" % args.lanes) if args.lanes > 1
             else "k_verify",
             "kernel_ms": round(kernel_ms, 4),

@@ -40,6 +40,151 @@ __device__ __forceinline__ void prod24(uint32_t* p, const uint32_t* a, const uin
     }
 }
 
+#define BLS_SUB13_12(m, s)                                                                                 \
+    asm("sub.cc.u32 %0, %0, %13;\n\t"                                                                     \
+        "subc.cc.u32 %1, %1, %14;\n\t"                                                                    \
+        "subc.cc.u32 %2, %2, %15;\n\t"                                                                    \
+        "subc.cc.u32 %3, %3, %16;\n\t"                                                                    \
+        "subc.cc.u32 %4, %4, %17;\n\t"                                                                    \
+        "subc.cc.u32 %5, %5, %18;\n\t"                                                                    \
+        "subc.cc.u32 %6, %6, %19;\n\t"                                                                    \
+        "subc.cc.u32 %7, %7, %20;\n\t"                                                                    \
+        "subc.cc.u32 %8, %8, %21;\n\t"                                                                    \
+        "subc.cc.u32 %9, %9, %22;\n\t"                                                                    \
+        "subc.cc.u32 %10, %10, %23;\n\t"                                                                  \
+        "subc.cc.u32 %11, %11, %24;\n\t"                                                                  \
+        "subc.u32 %12, %12, 0;"                                                                          \
+        : "+r"(m[0]), "+r"(m[1]), "+r"(m[2]), "+r"(m[3]), "+r"(m[4]), "+r"(m[5]), "+r"(m[6]), "+r"(m[7]),  \
+          "+r"(m[8]), "+r"(m[9]), "+r"(m[10]), "+r"(m[11]), "+r"(m[12])                                  \
+        : "r"((s)[0]), "r"((s)[1]), "r"((s)[2]), "r"((s)[3]), "r"((s)[4]), "r"((s)[5]), "r"((s)[6]),       \
+          "r"((s)[7]), "r"((s)[8]), "r"((s)[9]), "r"((s)[10]), "r"((s)[11]))
+#define BLS_ADD_MID(p, m)                                                                                    \
+    asm("add.cc.u32 %0, %0, %18;\n\t"                                                                     \
+        "addc.cc.u32 %1, %1, %19;\n\t"                                                                    \
+        "addc.cc.u32 %2, %2, %20;\n\t"                                                                    \
+        "addc.cc.u32 %3, %3, %21;\n\t"                                                                    \
+        "addc.cc.u32 %4, %4, %22;\n\t"                                                                    \
+        "addc.cc.u32 %5, %5, %23;\n\t"                                                                    \
+        "addc.cc.u32 %6, %6, %24;\n\t"                                                                    \
+        "addc.cc.u32 %7, %7, %25;\n\t"                                                                    \
+        "addc.cc.u32 %8, %8, %26;\n\t"                                                                    \
+        "addc.cc.u32 %9, %9, %27;\n\t"                                                                    \
+        "addc.cc.u32 %10, %10, %28;\n\t"                                                                  \
+        "addc.cc.u32 %11, %11, %29;\n\t"                                                                  \
+        "addc.cc.u32 %12, %12, %30;\n\t"                                                                  \
+        "addc.cc.u32 %13, %13, 0;\n\t"                                                                    \
+        "addc.cc.u32 %14, %14, 0;\n\t"                                                                    \
+        "addc.cc.u32 %15, %15, 0;\n\t"                                                                    \
+        "addc.cc.u32 %16, %16, 0;\n\t"                                                                    \
+        "addc.u32 %17, %17, 0;"                                                                          \
+        : "+r"((p)[6]), "+r"((p)[7]), "+r"((p)[8]), "+r"((p)[9]), "+r"((p)[10]), "+r"((p)[11]),            \
+          "+r"((p)[12]), "+r"((p)[13]), "+r"((p)[14]), "+r"((p)[15]), "+r"((p)[16]), "+r"((p)[17]),        \
+          "+r"((p)[18]), "+r"((p)[19]), "+r"((p)[20]), "+r"((p)[21]), "+r"((p)[22]), "+r"((p)[23])         \
+        : "r"(m[0]), "r"(m[1]), "r"(m[2]), "r"(m[3]), "r"(m[4]), "r"(m[5]), "r"(m[6]), "r"(m[7]),         \
+          "r"(m[8]), "r"(m[9]), "r"(m[10]), "r"(m[11]), "r"(m[12]))
+
+// t[0..5] += lo(a[0..5] * b), carry into t[6]
+__device__ __forceinline__ void chain_lo6(uint32_t* t, const uint32_t* a, uint32_t b) {
+    asm("mad.lo.cc.u32 %0, %7, %13, %0;\n\t"
+        "madc.lo.cc.u32 %1, %8, %13, %1;\n\t"
+        "madc.lo.cc.u32 %2, %9, %13, %2;\n\t"
+        "madc.lo.cc.u32 %3, %10, %13, %3;\n\t"
+        "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"
+        "madc.lo.cc.u32 %5, %12, %13, %5;\n\t"
+        "addc.u32 %6, %6, 0;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(b));
+}
+// t[1..6] += hi(a[0..5] * b); no carry leaves t[6]
+__device__ __forceinline__ void chain_hi6(uint32_t* t, const uint32_t* a, uint32_t b) {
+    asm("mad.hi.cc.u32 %0, %6, %12, %0;\n\t"
+        "madc.hi.cc.u32 %1, %7, %12, %1;\n\t"
+        "madc.hi.cc.u32 %2, %8, %12, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"
+        "madc.hi.cc.u32 %4, %10, %12, %4;\n\t"
+        "madc.hi.u32 %5, %11, %12, %5;"
+        : "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(b));
+}
+// r[0..11] = a[0..5] * b[0..5] (rows as in prod24)
+__device__ __forceinline__ void mul6(uint32_t* r, const uint32_t* a, const uint32_t* b) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) r[j] = a[j] * b[0];
+    asm("mad.hi.cc.u32 %0, %6, %12, %0;\n\t"
+        "madc.hi.cc.u32 %1, %7, %12, %1;\n\t"
+        "madc.hi.cc.u32 %2, %8, %12, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"
+        "madc.hi.cc.u32 %4, %10, %12, %4;\n\t"
+        "madc.hi.u32 %5, %11, %12, 0;"
+        : "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "=r"(r[6])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(b[0]));
+#pragma unroll
+    for (int i = 7; i < 12; ++i) r[i] = 0;
+#pragma unroll
+    for (int i = 1; i < 6; ++i) {
+        chain_lo6(r + i, a, b[i]);
+        chain_hi6(r + i, a, b[i]);
+    }
+}
+
+// p[0..23] = a * b by one level of Karatsuba on 6-limb halves: L = a0 b0,
+// H = a1 b1, M = (a0 + a1)(b0 + b1) with the halves' carry bits folded in,
+// p = L + (M - L - H) 2^192 + H 2^384.  Three 6 x 6 products (216 multiply
+// instructions) instead of 288; the sums and corrections are plain adds.
+__device__ __forceinline__ void prod24k(uint32_t* p, const uint32_t* a, const uint32_t* b) {
+    mul6(p, a, b);
+    mul6(p + 12, a + 6, b + 6);
+    uint32_t sa[6], sb[6], ca, cb;
+    asm("add.cc.u32 %0, %7, %13;\n\t"
+        "addc.cc.u32 %1, %8, %14;\n\t"
+        "addc.cc.u32 %2, %9, %15;\n\t"
+        "addc.cc.u32 %3, %10, %16;\n\t"
+        "addc.cc.u32 %4, %11, %17;\n\t"
+        "addc.cc.u32 %5, %12, %18;\n\t"
+        "addc.u32 %6, 0, 0;"
+        : "=r"(sa[0]), "=r"(sa[1]), "=r"(sa[2]), "=r"(sa[3]), "=r"(sa[4]), "=r"(sa[5]), "=r"(ca)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]),
+          "r"(a[6]), "r"(a[7]), "r"(a[8]), "r"(a[9]), "r"(a[10]), "r"(a[11]));
+    asm("add.cc.u32 %0, %7, %13;\n\t"
+        "addc.cc.u32 %1, %8, %14;\n\t"
+        "addc.cc.u32 %2, %9, %15;\n\t"
+        "addc.cc.u32 %3, %10, %16;\n\t"
+        "addc.cc.u32 %4, %11, %17;\n\t"
+        "addc.cc.u32 %5, %12, %18;\n\t"
+        "addc.u32 %6, 0, 0;"
+        : "=r"(sb[0]), "=r"(sb[1]), "=r"(sb[2]), "=r"(sb[3]), "=r"(sb[4]), "=r"(sb[5]), "=r"(cb)
+        : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]),
+          "r"(b[6]), "r"(b[7]), "r"(b[8]), "r"(b[9]), "r"(b[10]), "r"(b[11]));
+    uint32_t m[13];
+    mul6(m, sa, sb);
+    // + ca sb 2^192 + cb sa 2^192 + ca cb 2^384 (m stays below 2^386)
+    const uint32_t ma = 0u - ca, mb = 0u - cb;
+    asm("add.cc.u32 %0, %0, %7;\n\t"
+        "addc.cc.u32 %1, %1, %8;\n\t"
+        "addc.cc.u32 %2, %2, %9;\n\t"
+        "addc.cc.u32 %3, %3, %10;\n\t"
+        "addc.cc.u32 %4, %4, %11;\n\t"
+        "addc.cc.u32 %5, %5, %12;\n\t"
+        "addc.u32 %6, %13, 0;"
+        : "+r"(m[6]), "+r"(m[7]), "+r"(m[8]), "+r"(m[9]), "+r"(m[10]), "+r"(m[11]), "=r"(m[12])
+        : "r"(sb[0] & ma), "r"(sb[1] & ma), "r"(sb[2] & ma), "r"(sb[3] & ma), "r"(sb[4] & ma), "r"(sb[5] & ma),
+          "r"(ca & cb));
+    asm("add.cc.u32 %0, %0, %7;\n\t"
+        "addc.cc.u32 %1, %1, %8;\n\t"
+        "addc.cc.u32 %2, %2, %9;\n\t"
+        "addc.cc.u32 %3, %3, %10;\n\t"
+        "addc.cc.u32 %4, %4, %11;\n\t"
+        "addc.cc.u32 %5, %5, %12;\n\t"
+        "addc.u32 %6, %6, 0;"
+        : "+r"(m[6]), "+r"(m[7]), "+r"(m[8]), "+r"(m[9]), "+r"(m[10]), "+r"(m[11]), "+r"(m[12])
+        : "r"(sa[0] & mb), "r"(sa[1] & mb), "r"(sa[2] & mb), "r"(sa[3] & mb), "r"(sa[4] & mb), "r"(sa[5] & mb));
+    // m -= L, m -= H: a0 b1 + a1 b0, below 2^385
+    BLS_SUB13_12(m, p);
+    BLS_SUB13_12(m, p + 12);
+    // p[6..23] += m[0..12]
+    BLS_ADD_MID(p, m);
+}
+
 // acc[12..25] += x (neg = 0) or -= x (neg = 1): acc += +-x 2^384, modulo 2^832
 __device__ __forceinline__ void acc_add_hi(uint32_t* acc, const uint32_t* x, uint32_t neg) {
     uint32_t c = neg, m = 0u - neg;

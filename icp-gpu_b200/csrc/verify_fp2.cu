@@ -184,7 +184,7 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
             } else {                        // NORM: x_j^2
                 load_fp(V, sm, xs, j);
             }
-            f2::prod24(P, U, V);
+            f2::prod24k(P, U, V);
             acc_pair(accO, accX, P, (cw >> (c0 + 4 * j)) & 3u, (cw >> (c1 + 4 * j)) & 3u);
         }
     }
@@ -511,8 +511,8 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
 size_t smem_bytes() { return (size_t)(kSlotArea + kXchArea + kFlagArea) * 4; }
 
 // The carry-chain ceiling the verify kernel is measured against: every thread
-// runs `iters` 12 x 12-limb products (prod24: 144 mul.lo + 144 mul.hi chained
-// through the carry flag, 288 IMAD-pipe instructions) and adds each into a
+// runs `iters` schoolbook 12 x 12-limb products (prod24: 144 mul.lo + 144
+// mul.hi chained through the carry flag, 288 IMAD-pipe instructions) and adds each into a
 // 26-limb accumulator, with the verify kernel's block shape and occupancy and
 // no loads, barriers or reductions; one operand changes every iteration so
 // no product can be hoisted.

@@ -129,3 +129,22 @@ def test_generated_header_is_current():
         fresh = open(tf.name).read()
     os.unlink(tf.name)
     assert open(path).read() == fresh
+
+
+def test_bench_counts_match_the_sequence():
+    """The own-work figures bench.py reports are the generated sequence's."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    progs = {i: fn() for i, (name, fn, _) in enumerate(G.PROGRAMS)}
+    prods = redcs = 0
+    for code, d, a, b, ci in G.driver_sequence(True):
+        if code & G.COND_ML or code >= len(G.PROGRAMS):
+            continue
+        for o in progs[code]:
+            if o is None:
+                continue
+            prods += G.half_products(o, 0) + G.half_products(o, 1)
+            redcs += 2 if o.mode in (G.M_SIMPLE, G.M_FULL) else 0
+    assert (prods, redcs) == (bench.OWN_PRODUCTS_PER_VERIFY, bench.OWN_REDC_PER_VERIFY)
