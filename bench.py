@@ -310,7 +310,10 @@ def run_gpu(args):
 
     chain_timad = ctx.imad_chain_rate() / 1e12
     batching = serving = ingest = hashing = rlc = None
-    if not args.no_extras:
+    # the single-GPU sections (ingest, hashing, random linear combinations,
+    # batching, serving) run on one GPU only; under torchrun every rank times
+    # the headline step alone
+    if not args.no_extras and world == 1:
         sizes = [int(v) for v in args.ingest_keys.split(",") if int(v) > 0]
         ingest = [run_ingest(G, WL, local, args.lanes, k) for k in sizes] or None
         hashing = run_hash(G, WL, ctx, wl, pk_ids)
