@@ -500,7 +500,8 @@ def run_rlc(G, WL, ctx, wl4096, pk_ids4096, n=65536, reps=3):
             "fallback_4096_ms": round(t_fb * 1e3, 2), "per_item_4096_ms": round(t_fb_item * 1e3, 2)}
 
 
-def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ring", ring_blocks_per_sm=0):
+def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ring", ring_blocks_per_sm=0,
+                ring_blocks=0):
     """Serving workload: seeded Poisson stream of requests (sizes log-uniform in
     [1, 512]) over a pool of 40 resident keys, through the continuous-batching
     server (bls_server_*) under a 4 GiB device-memory cap: `mode` "ring" (one
@@ -524,7 +525,7 @@ def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ri
 
     if mode == "ring":
         server = G.Server(ctx, max_batch_items=512, mem_cap_bytes=4 << 30, mode=G.SERVE_RING,
-                          ring_blocks_per_sm=ring_blocks_per_sm)
+                          ring_blocks_per_sm=ring_blocks_per_sm, ring_blocks=ring_blocks)
     else:
         server = G.Server(ctx, slots=slots, max_batch_items=max_batch, mem_cap_bytes=4 << 30)
     with server as srv:

@@ -63,7 +63,7 @@ MODE_PLAIN, MODE_PERSISTENT = 0, 1
 class ServerConfig(ctypes.Structure):
     _fields_ = [("sig_format", ctypes.c_int), ("slots", ctypes.c_int), ("max_batch_items", ctypes.c_int),
                 ("mem_cap_bytes", ctypes.c_size_t), ("mode", ctypes.c_int), ("ring_items", ctypes.c_int),
-                ("ring_blocks_per_sm", ctypes.c_int)]
+                ("ring_blocks_per_sm", ctypes.c_int), ("ring_blocks", ctypes.c_int)]
 
 
 SERVE_SLOTS = 0
@@ -429,9 +429,9 @@ class Server:
     """Continuous-batching verify server on a Context (bls_server_*)."""
 
     def __init__(self, ctx, compressed=False, slots=0, max_batch_items=0, mem_cap_bytes=0, mode=SERVE_SLOTS,
-                 ring_items=0, ring_blocks_per_sm=0):
+                 ring_items=0, ring_blocks_per_sm=0, ring_blocks=0):
         cfg = ServerConfig(SIG_COMPRESSED if compressed else SIG_AFFINE, slots, max_batch_items, mem_cap_bytes, mode,
-                           ring_items, ring_blocks_per_sm)
+                           ring_items, ring_blocks_per_sm, ring_blocks)
         h = ctypes.c_void_p()
         rc = ctx.lib.bls_server_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h))
         if rc != BLS_OK:

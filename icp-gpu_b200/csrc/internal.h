@@ -83,7 +83,7 @@ cudaError_t launch_lines_normalize(const uint64_t* raw, int n, uint64_t* norm, u
 // per-Fp programs (verify_vm.cu).
 cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int blocks_per_sm,
                                 int sms, cudaStream_t s);
-cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks_per_sm, int sms, cudaStream_t s);
+cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks, int sms, cudaStream_t s);
 cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, int blocks_per_sm, int sms,
                               cudaStream_t s);
 size_t verify_fp2_smem_bytes();

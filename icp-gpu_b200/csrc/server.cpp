@@ -199,7 +199,8 @@ struct bls_server {
         a.serve_cap = ring.cap;
         a.serve_idle_ns = 20ull * 1000 * 1000;
         a.serve_max_ns = 60ull * 1000 * 1000 * 1000;
-        if (bls::launch_verify_fp2_serve(a, cfg.ring_blocks_per_sm, view.sms, ring.kern) ||
+        const int blocks = cfg.ring_blocks > 0 ? cfg.ring_blocks : cfg.ring_blocks_per_sm * view.sms;
+        if (bls::launch_verify_fp2_serve(a, blocks, view.sms, ring.kern) ||
             cudaEventRecord(ring.done, ring.kern))
             return BLS_ERR_CUDA;
         ring.launched = true;
@@ -390,7 +391,7 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
     if ((s->cfg.sig_format != BLS_SIG_AFFINE && s->cfg.sig_format != BLS_SIG_COMPRESSED) ||
         (s->cfg.mode != BLS_SERVE_SLOTS && s->cfg.mode != BLS_SERVE_RING) ||
         (s->cfg.mode == BLS_SERVE_RING && s->cfg.sig_format != BLS_SIG_AFFINE) || s->cfg.ring_items < 0 ||
-        s->cfg.ring_blocks_per_sm < 0) {
+        s->cfg.ring_blocks_per_sm < 0 || s->cfg.ring_blocks < 0) {
         delete s;
         return BLS_ERR_INVALID;
     }

@@ -582,15 +582,16 @@ cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s
     return e;
 }
 
-// ring serving: one persistent block per resident slot
-cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks_per_sm, int sms, cudaStream_t s) {
-    if (!a.serve_avail || !a.serve_stop || !a.serve_claimed || a.serve_cap == 0 || a.serve_cap % kPairsPerBlock)
+// ring serving: `blocks` persistent blocks (at most the resident slots)
+cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks, int sms, cudaStream_t s) {
+    if (!a.serve_avail || !a.serve_stop || !a.serve_claimed || a.serve_cap == 0 || a.serve_cap % kPairsPerBlock ||
+        blocks <= 0)
         return cudaErrorInvalidValue;
     cudaError_t e = configure();
     if (e != cudaSuccess) return e;
     const int res = resident();
-    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm : (res > 0 ? res : 1);
-    k_verify_fp2<<<per_sm * sms, kThreads, smem_bytes(), s>>>(a, nullptr);
+    if (res > 0 && blocks > res * sms) blocks = res * sms;
+    k_verify_fp2<<<blocks, kThreads, smem_bytes(), s>>>(a, nullptr);
     return cudaGetLastError();
 }
 

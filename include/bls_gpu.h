@@ -229,6 +229,8 @@ typedef struct {
     int ring_items;            /* ring mode: ring slots, rounded up to a multiple of 5 (0 = 65535) */
     int ring_blocks_per_sm;    /* ring mode: resident blocks of the kernel per SM (0 = 4); fewer
                                   verifications share an SM, so each finishes sooner */
+    int ring_blocks;           /* ring mode: total resident blocks, overriding ring_blocks_per_sm
+                                  when > 0 (capped at what the device holds) */
 } bls_server_config;
 
 /* Serving modes.  SLOTS: the launch slots above.  RING (affine signatures,
