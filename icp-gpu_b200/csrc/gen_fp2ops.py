@@ -817,6 +817,10 @@ def emit(path):
     L.append("constexpr uint32_t kOpLoadCorr = %d, kOpMillerDone = %d, kOpLoadLines = %d, kCondMl = 0x%xu;"
              % (OP_LOAD_CORR, OP_MILLER_DONE, OP_LOAD_LINES, COND_ML))
     L.append("constexpr int kTGroup = %d;" % T_GROUP)
+    max_bias = max(b for name, fn, _ in PROGRAMS for o in fn() if o is not None
+                   for b in (o.bias_re, o.bias_im, o.bias_lin_re, o.bias_lin_im))
+    L.append("// largest bias multiple k of any output (the kernel keeps k p for k = 0 .. kMaxBias)")
+    L.append("constexpr int kMaxBias = %d;" % max_bias)
     seqs = [driver_sequence(False), driver_sequence(True)]
     L.append("// Fp12 groups the sequences touch (operands, results, the inverse's temporaries)")
     L.append("constexpr int kGroupsUsed = %d;" % groups_used(seqs))

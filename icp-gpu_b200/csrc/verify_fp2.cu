@@ -20,7 +20,8 @@
 // Shared memory: 8 block-shared constant slots (0, 1, Frobenius constants),
 // then per pairing kGroups groups of 6 Fp2 slots and a 12-slot C area (lines,
 // points), then the exchange area (per pairing and coefficient, one 26-word
-// partial sum per half) and per-pairing flags.  An Fp2 slot is 24 words: re
+// partial sum per half), per-pairing flags and the table of k p for the
+// outputs' bias multiples.  An Fp2 slot is 24 words: re
 // then im, each below 2^381 + p.  Every program accumulates, exchanges, meets,
 // reduces, meets, writes and meets again, so a program may overwrite its own
 // inputs.
@@ -45,6 +46,9 @@ constexpr int kSlotArea = (kKSlots + kPairsPerBlock * kPairSlots) * kSlotWords; 
 constexpr int kXchWords = 28;                   // 26 used; 112 B keeps uint4 alignment
 constexpr int kXchArea = kPairsPerBlock * kLanes * 2 * kXchWords;                 // words
 constexpr int kFlagArea = kPairsPerBlock * 2 + 2;                                // words
+constexpr int kKpCount = f2::kMaxBias + 1;      // k p for every bias multiple k, 16 words each
+static_assert(kKpCount <= kThreads, "one thread per table entry at start-up");
+
 
 struct Ctx {
     uint32_t* sm;      // shared memory (words): slots, then exchange, then flags
@@ -81,6 +85,18 @@ __device__ __forceinline__ void store_fp(uint32_t* sm, uint32_t slot, int comp, 
     s[2] = make_uint4(x[8], x[9], x[10], x[11]);
 }
 
+// t[0..12] = k p from the block's table (16 words per entry, filled at the
+// kernel's start; k <= kMaxBias for every descriptor the generator writes)
+__device__ __forceinline__ void load_kp(uint32_t* t, const uint32_t* sm, uint32_t k) {
+    const uint32_t* e = sm + kSlotArea + kXchArea + kFlagArea + 16 * k;
+    const uint4* v = reinterpret_cast<const uint4*>(e);
+    const uint4 a = v[0], b = v[1], c = v[2];
+    t[0] = a.x; t[1] = a.y; t[2] = a.z; t[3] = a.w;
+    t[4] = b.x; t[5] = b.y; t[6] = b.z; t[7] = b.w;
+    t[8] = c.x; t[9] = c.y; t[10] = c.z; t[11] = c.w;
+    t[12] = e[12];
+}
+
 __device__ __forceinline__ int sext4(uint32_t v) { return (int)(v << 28) >> 28; }
 
 // P into the two accumulators with coefficients ca, cb (bit 0 nonzero, bit 1 negative)
@@ -109,8 +125,8 @@ __device__ __forceinline__ void accumulate(uint32_t off, uint32_t* sm, const Bas
 #pragma unroll
     for (int i = 0; i < 12; ++i) accO[i] = accX[i] = 0;
     accO[25] = accX[25] = 0;
-    f2::set_kp(accO + 12, (bias >> sw) & 0xffu);
-    f2::set_kp(accX + 12, (bias >> (8u - sw)) & 0xffu);
+    load_kp(accO + 12, sm, (bias >> sw) & 0xffu);
+    load_kp(accX + 12, sm, (bias >> (8u - sw)) & 0xffu);
     for (uint32_t t = 0; t < nt; ++t) {
         const uint32_t w = f2::kDesc[off + 2 + t];
         const uint32_t kind = w & 7u, xi = (w >> 3) & 1u, neg = (w >> 4) & 1u, dbl = (w >> 5) & 1u,
@@ -222,7 +238,7 @@ __device__ __forceinline__ void finish(uint32_t off, const uint32_t* sm, const B
     }
     uint32_t r[13];
     if (mode == f2::kModeLin) {
-        f2::set_kp(r, bias_lin);
+        load_kp(r, sm, bias_lin);
         for (uint32_t j = 0; j < nl; ++j) {
             uint32_t z[12];
             load_fp(z, sm, slot_addr(bs, lin[j] >> 8), half);
@@ -248,7 +264,7 @@ __device__ __forceinline__ void finish(uint32_t off, const uint32_t* sm, const B
         }
         uint32_t q[12];
         f2::qp_reduce(q, red);
-        f2::set_kp(r, bias_lin);
+        load_kp(r, sm, bias_lin);
         f2::madd13(r, q, cc);
         for (uint32_t j = 0; j < nl; ++j) {
             uint32_t z[12];
@@ -396,6 +412,12 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
     const int pi = lane32 / kLanes;
 
     for (int i = threadIdx.x; i < kKSlots * kSlotWords; i += blockDim.x) sm[i] = f2::kKSlots[i / kSlotWords][i % kSlotWords];
+    if (threadIdx.x < kKpCount) {
+        uint32_t t[13];
+        f2::set_kp(t, threadIdx.x);
+#pragma unroll
+        for (int i = 0; i < 13; ++i) sm[kSlotArea + kXchArea + kFlagArea + 16 * threadIdx.x + i] = t[i];
+    }
     __syncthreads();
 
     Ctx c;
@@ -508,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
     }
 }
 
-size_t smem_bytes() { return (size_t)(kSlotArea + kXchArea + kFlagArea) * 4; }
+size_t smem_bytes() { return (size_t)(kSlotArea + kXchArea + kFlagArea + 16 * kKpCount) * 4; }
 
 // The carry-chain ceiling the verify kernel is measured against: every thread
 // runs `iters` schoolbook 12 x 12-limb products (prod24: 144 mul.lo + 144
