@@ -383,25 +383,51 @@ __device__ __forceinline__ void qp_reduce(uint32_t* out, const uint32_t* v) {
     (void)top;  // zero: v - QP[h] < 2^384
 }
 
-// t (13 limbs) += c * x (x 12 limbs, |c| small), modulo 2^416
+// t[0..12] += c x (x: 12 limbs, |c| < 2^31), modulo 2^416: y = |c| x by
+// shifts for |c| <= 2 (the common 1 and 2 of the programs' linear terms) or
+// by one multiply chain, then one add chain of y or of its complement (no
+// branch on the sign, which differs between lanes)
 __device__ __forceinline__ void madd13(uint32_t* t, const uint32_t* x, int c) {
-    if (c >= 0) {
-        chain_lo(t, x, (uint32_t)c);
-        chain_hi(t, x, (uint32_t)c);
-    } else {
-        uint32_t u[13];
+    const uint32_t a = (uint32_t)(c < 0 ? -c : c), m = c < 0 ? 0xffffffffu : 0u;
+    uint32_t y[13];
+    if (a <= 2u) {
 #pragma unroll
-        for (int i = 0; i < 13; ++i) u[i] = 0;
-        chain_lo(u, x, (uint32_t)(-c));
-        chain_hi(u, x, (uint32_t)(-c));
-        uint32_t b = 0;
+        for (int i = 0; i < 12; ++i) y[i] = x[i];
+        y[12] = 0;
+        if (a == 2u) {
+            y[12] = x[11] >> 31;
 #pragma unroll
-        for (int i = 0; i < 13; ++i) {
-            uint64_t d = (uint64_t)t[i] - u[i] - b;
-            t[i] = (uint32_t)d;
-            b = (uint32_t)(d >> 63);
+            for (int i = 11; i > 0; --i) y[i] = __funnelshift_l(x[i - 1], x[i], 1);
+            y[0] = x[0] << 1;
+        } else if (a == 0u) {
+            return;
         }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 13; ++i) y[i] = 0;
+        chain_lo(y, x, a);
+        chain_hi(y, x, a);
     }
+    uint32_t cf;   // carry in = 1 for a subtraction: m + m carries out exactly when m is all ones
+    asm("add.cc.u32 %13, %27, %27;\n\t"
+        "addc.cc.u32 %0, %0, %14;\n\t"
+        "addc.cc.u32 %1, %1, %15;\n\t"
+        "addc.cc.u32 %2, %2, %16;\n\t"
+        "addc.cc.u32 %3, %3, %17;\n\t"
+        "addc.cc.u32 %4, %4, %18;\n\t"
+        "addc.cc.u32 %5, %5, %19;\n\t"
+        "addc.cc.u32 %6, %6, %20;\n\t"
+        "addc.cc.u32 %7, %7, %21;\n\t"
+        "addc.cc.u32 %8, %8, %22;\n\t"
+        "addc.cc.u32 %9, %9, %23;\n\t"
+        "addc.cc.u32 %10, %10, %24;\n\t"
+        "addc.cc.u32 %11, %11, %25;\n\t"
+        "addc.u32 %12, %12, %26;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]),
+          "+r"(t[8]), "+r"(t[9]), "+r"(t[10]), "+r"(t[11]), "+r"(t[12]), "=r"(cf)
+        : "r"(y[0] ^ m), "r"(y[1] ^ m), "r"(y[2] ^ m), "r"(y[3] ^ m), "r"(y[4] ^ m), "r"(y[5] ^ m), "r"(y[6] ^ m),
+          "r"(y[7] ^ m), "r"(y[8] ^ m), "r"(y[9] ^ m), "r"(y[10] ^ m), "r"(y[11] ^ m), "r"(y[12] ^ m), "r"(m));
+    (void)cf;
 }
 
 // r = a + b (12 limbs, no carry out: both below 2^383)
