@@ -461,7 +461,7 @@ def run_hash(G, WL, ctx, wl, pk_ids, reps=3):
     t_gpu_hash = best(lambda: ctx.neg_hash_to_g1(msgs, WL.DST))
     t_cpu_hash = best(lambda: WL.g1_neg(WL.hash_to_g1(msgs)))
     t_verify = best(lambda: ctx.verify(wl["sigs"], wl["nhms"], pk_ids))
-    return {"items": n, "suite": "RFC 9380 hash_to_curve, expand_message_xmd SHA-256, SVDW map",
+    return {"items": n, "suite": "RFC 9380 hash_to_curve, expand_message_xmd SHA-256, SSWU map + 11-isogeny",
             "verify_messages_per_s": round(n / t_msgs, 1),
             "verify_messages_api": "bls_verify_messages (hash + verify on the GPU, host buffers)",
             "cpu_hash_then_verify_per_s": round(n / (t_cpu_hash + t_verify), 1),

@@ -352,7 +352,7 @@ class Context:
         return self.lib.bls_ctx_stream(self.h)
 
     def neg_hash_to_g1(self, msgs, dst):
-        """-H(m) for each message (RFC 9380 hash_to_curve, SVDW suite) on the GPU: (n, 12) u64."""
+        """-H(m) for each message (RFC 9380 hash_to_curve, SSWU suite) on the GPU: (n, 12) u64."""
         buf, off = pack_messages(msgs)
         d = np.frombuffer(bytes(dst), dtype=np.uint8).copy()
         out = np.zeros((len(msgs), 12), dtype=np.uint64)

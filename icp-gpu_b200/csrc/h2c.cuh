@@ -1,13 +1,13 @@
-// Hash to G1 on the device: RFC 9380 hash_to_curve for BLS12-381 G1 with
-// expand_message_xmd over SHA-256 and the Shallue-van de Woestijne map
-// (section 6.6.1) on y^2 = x^3 + 4, then cofactor clearing by h_eff = 1 - x.
-// The reference's callers hash on the CPU per item with ic_bls12_381's
-// hash_to_curve (ic-integration/patches/ic-gpu-consensus.patch:454-457,
-// ic-bench/src/main.rs:65-76), whose suite maps with SSWU on an 11-isogenous
-// curve; the isogeny's constants are not restated here, so this hash is the
-// SVDW suite of the same RFC and gives different points than ic_bls12_381's.
-// Constants from gen_h2c.py (h2c.inc); the kernel (hash.cu) runs the two maps
-// of a message on two threads.
+// Hash to G1 on the device: RFC 9380 hash_to_curve for BLS12-381 G1, the
+// suite BLS12381G1_XMD:SHA-256_SSWU_RO_ that ic_bls12_381's hash_to_curve
+// implements and the reference's callers run on the CPU per item
+// (ic-integration/patches/ic-gpu-consensus.patch:454-457,
+// ic-bench/src/main.rs:65-76): expand_message_xmd over SHA-256, two field
+// elements, the simplified SWU map (section 6.6.2) on the 11-isogenous curve
+// E' and the 11-isogeny to y^2 = x^3 + 4 (section 6.6.3), point addition,
+// cofactor clearing by h_eff = 1 - x.  Constants from gen_h2c.py (h2c.inc),
+// which derives the isogeny; the kernel (hash.cu) runs the two maps of a
+// message on two threads.
 #pragma once
 #include "g1.cuh"
 #include "h2c.inc"
@@ -131,33 +131,52 @@ static __device__ __noinline__ fp fp_inv0(const fp& a) {   // 0 for 0 (RFC 9380 
 
 __device__ __forceinline__ uint32_t sgn0(const fp& a) { return fp_from_mont(a).w[0] & 1u; }
 
-__device__ __forceinline__ fp g_of(const fp& x) { return fp_add(fp_mul(fp_sqr(x), x), fp_four()); }
+// g'(x) = x^3 + A' x + B' on E'
+__device__ __forceinline__ fp g_iso(const fp& x) {
+    return fp_add(fp_mul(fp_add(fp_sqr(x), fp_load_u64(kIsoA)), x), fp_load_u64(kIsoB));
+}
 
-// the SVDW map, RFC 9380 section 6.6.1 (A = 0, B = 4); square roots by
-// a^((p+1)/4), tested by squaring
-static __device__ __noinline__ void map_svdw(const fp& u, fp& x, fp& y) {
-    const fp one = fp_one();
-    fp tv1 = fp_mul(fp_sqr(u), fp_load_u64(kC1));
-    const fp tv2 = fp_add(one, tv1);
-    tv1 = fp_sub(one, tv1);
-    const fp tv3 = fp_inv0(fp_mul(tv1, tv2));
-    const fp tv4 = fp_mul(fp_mul(fp_mul(u, tv1), tv3), fp_load_u64(kC3));
-    const fp c2 = fp_load_u64(kC2);
-    x = fp_sub(c2, tv4);
-    fp gx = g_of(x);
-    y = fp_sqrt_candidate(gx);
-    if (!fp_eq(fp_sqr(y), gx)) {
-        x = fp_add(c2, tv4);
-        gx = g_of(x);
-        y = fp_sqrt_candidate(gx);
-        if (!fp_eq(fp_sqr(y), gx)) {
-            fp x3 = fp_mul(fp_sqr(tv2), tv3);
-            x3 = fp_mul(fp_sqr(x3), fp_load_u64(kC4));
-            x = fp_add(x3, fp_load_u64(kZ));
-            y = fp_sqrt_candidate(g_of(x));   // a square by construction of Z
-        }
+// the simplified SWU map to E', RFC 9380 section 6.6.2: x1 = (-B'/A')
+// (1 + 1 / (Z^2 u^4 + Z u^2)) (B' / (Z A') when that sum is 0), x2 = Z u^2 x1;
+// x1 when g'(x1) is a square, else x2 (then g'(x2) is one, by the choice of
+// Z); square roots by a^((p+1)/4), tested by squaring; sgn0(y) = sgn0(u)
+static __device__ __noinline__ void map_sswu(const fp& u, fp& x, fp& y) {
+    const fp zu2 = fp_mul(fp_load_u64(kZ), fp_sqr(u));
+    const fp tv1 = fp_add(fp_sqr(zu2), zu2);
+    fp x1;
+    if (fp_is_zero(tv1)) {
+        x1 = fp_load_u64(kSswuC2);
+    } else {
+        x1 = fp_mul(fp_load_u64(kSswuC1), fp_add(fp_one(), fp_inv0(tv1)));
+    }
+    const fp gx1 = g_iso(x1);
+    x = x1;
+    y = fp_sqrt_candidate(gx1);
+    if (!fp_eq(fp_sqr(y), gx1)) {
+        x = fp_mul(zu2, x1);
+        y = fp_sqrt_candidate(g_iso(x));
     }
     if (sgn0(u) != sgn0(y)) y = fp_neg(y);
+}
+
+// c(x) by Horner over `len` coefficients of 6 u64 (Montgomery), plus x^len
+// when `monic`
+__device__ __forceinline__ fp horner(const uint64_t* c, int len, bool monic, const fp& x) {
+    fp acc = monic ? fp_one() : fp_load_u64(c + 6 * (len - 1));
+    for (int i = monic ? len - 1 : len - 2; i >= 0; --i) acc = fp_add(fp_mul(acc, x), fp_load_u64(c + 6 * i));
+    return acc;
+}
+
+// the 11-isogeny E' -> E (RFC 9380 section 6.6.3 with the map of appendix
+// E.2), one inversion for both denominators; the Jacobian identity when a
+// denominator vanishes
+static __device__ __noinline__ g1j iso_map(const fp& xs, const fp& ys) {
+    const fp xn = horner(kIsoXNum, kIsoXNumLen, false, xs), xd = horner(kIsoXDen, kIsoXDenLen, true, xs);
+    const fp yn = horner(kIsoYNum, kIsoYNumLen, false, xs), yd = horner(kIsoYDen, kIsoYDenLen, true, xs);
+    const fp den = fp_mul(xd, yd);
+    if (fp_is_zero(den)) return {fp_one(), fp_one(), fp_zero()};
+    const fp di = fp_inv0(den);
+    return {fp_mul(fp_mul(xn, yd), di), fp_mul(fp_mul(fp_mul(ys, yn), xd), di), fp_one()};
 }
 
 // affine (x, y) of a Jacobian point; false for the identity
@@ -169,12 +188,11 @@ __device__ __forceinline__ bool to_affine(const g1j& p, fp& x, fp& y) {
     return true;
 }
 
-// -H(msg) from the two mapped points (affine), as affine Montgomery (x, y);
-// the identity as x = 0, y = R mod p.  Q = P0 + P1 stays Jacobian through the
+// -H(msg) from the two mapped points, as affine Montgomery (x, y); the
+// identity as x = 0, y = R mod p.  Q = P0 + P1 stays Jacobian through the
 // cofactor clearing [h_eff] Q; one inversion at the end.
-static __device__ __noinline__ void neg_clear(const fp& x0, const fp& y0, const fp& x1, const fp& y1, fp& ox,
-                                              fp& oy) {
-    const g1j q = g1j_add_affine(g1j{x0, y0, fp_one()}, x1, y1);
+static __device__ __noinline__ void neg_clear(const g1j& p0, const g1j& p1, fp& ox, fp& oy) {
+    const g1j q = g1j_add(p0, p1);
     g1j r = q;
     for (int i = 62; i >= 0; --i) {
         r = g1j_dbl(r);

@@ -9,8 +9,9 @@ libbls_workload.so (C++, host CPU): the caller's side of the verify path.
 Definitions (one SplitMix64 stream per config seed):
   scalar   4 draws -> 255-bit little-endian integer, rejected unless in [1, r)
   message  4 draws -> 32 bytes (little-endian words)
-  H(m)     RFC 9380 hash_to_curve to G1, SHA-256 expander, DST below,
-           Shallue-van de Woestijne map
+  H(m)     RFC 9380 hash_to_curve to G1, suite BLS12381G1_XMD:SHA-256_SSWU_RO_
+           (ic_bls12_381's): SHA-256 expander, DST below, simplified SWU map
+           on the 11-isogenous curve, isogeny to E
   sig      sk * H(m);  the verifier receives -H(m') for the message it checks
 """
 import ctypes
@@ -20,7 +21,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-DST = b"BLS_BENCH_G1_XMD:SHA-256_SVDW_RO_"
+DST = b"BLS_BENCH_G1_XMD:SHA-256_SSWU_RO_"
 R_ORDER = 0x73eda753299d7d483339d80809a1d80553bda402fffe5bfeffffffff00000001
 P_MOD = 0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab
 M64 = (1 << 64) - 1

@@ -10,9 +10,11 @@
 //
 // Hash to G1 follows RFC 9380's hash_to_curve: expand_message_xmd with
 // SHA-256 (FIPS 180-4), hash_to_field (L = 64, two elements), map_to_curve,
-// point addition, clear_cofactor by h_eff = 1 - x.  The map is the
-// Shallue-van de Woestijne method of RFC 9380 section 6.6.1 (Z = -3 from
-// appendix H.1).
+// point addition, clear_cofactor by h_eff = 1 - x.  The map is the suite
+// BLS12381G1_XMD:SHA-256_SSWU_RO_ (ic_bls12_381's hash_to_curve): the
+// simplified SWU map of RFC 9380 section 6.6.2 on the 11-isogenous curve E'
+// and the 11-isogeny to E (section 6.6.3), with the constants that
+// csrc/gen_h2c.py derives (h2c.inc, host arrays here).
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -20,6 +22,9 @@
 #include <vector>
 
 typedef unsigned __int128 u128;
+
+#define BLS_H2C_CONST static const
+#include "../csrc/h2c.inc"
 
 namespace wl {
 
@@ -255,24 +260,17 @@ template <class T> bool to_affine(const Jac<T>& p, T& x, T& y) {
 }
 
 // ------------------------------------------------------------------ hash to G1
-struct Svdw { F z, c1, c2, c3, c4; };
-const Svdw& svdw() {
-    static const Svdw s = [] {
-        Svdw c;
-        c.z = neg(small(3));
-        F gz = add(mul(sqr(c.z), c.z), small(4));                     // g(Z) = Z^3 + 4
-        c.c1 = gz;
-        c.c2 = mul(neg(c.z), inv(small(2)));                          // -Z / 2
-        F t = mul(small(3), sqr(c.z));                                // 3 Z^2 (A = 0)
-        F c3 = sqrt_cand(neg(mul(gz, t)));                            // sqrt(-g(Z) (3 Z^2))
-        if (sgn0(c3)) c3 = neg(c3);
-        c.c3 = c3;
-        c.c4 = mul(neg(mul(small(4), gz)), inv(t));                   // -4 g(Z) / (3 Z^2)
-        return c;
-    }();
-    return s;
+inline F fconst(const uint64_t* c) { F r; memcpy(r.v, c, 48); return r; }
+inline F g_of(const F& x) { return add(mul(sqr(x), x), small(4)); }   // x^3 + 4 on E
+inline F g_iso(const F& x) {           // x^3 + A' x + B' on E'
+    return add(mul(add(sqr(x), fconst(bls::h2c::kIsoA)), x), fconst(bls::h2c::kIsoB));
 }
-inline F g_of(const F& x) { return add(mul(sqr(x), x), small(4)); }
+// coefficients c[0..len-1] by Horner, plus x^len when monic
+inline F horner(const uint64_t* c, int len, bool monic, const F& x) {
+    F acc = monic ? one() : fconst(c + 6 * (len - 1));
+    for (int i = monic ? len - 1 : len - 2; i >= 0; --i) acc = add(mul(acc, x), fconst(c + 6 * i));
+    return acc;
+}
 
 void expand_xmd(const uint8_t* msg, size_t mlen, const uint8_t* dst, size_t dlen, uint8_t* out, size_t len) {
     size_t ell = (len + 31) / 32;
@@ -323,33 +321,29 @@ F field_from_64(const uint8_t* b) {
     F b2 = to_mont(lo);
     return add(a, b2);
 }
-void map_svdw(const F& u, F& x, F& y) {
-    const Svdw& c = svdw();
-    F tv1 = mul(sqr(u), c.c1);
-    F tv2 = add(one(), tv1);
-    tv1 = sub(one(), tv1);
-    F tv3 = inv(mul(tv1, tv2));
-    F tv4 = mul(mul(mul(u, tv1), tv3), c.c3);
-    F x1 = sub(c.c2, tv4);
-    bool e1 = is_square(g_of(x1));
-    F x2 = add(c.c2, tv4);
-    bool e2 = is_square(g_of(x2)) && !e1;
-    F x3 = mul(sqr(mul(sqr(tv2), tv3)), c.c4);
-    x3 = add(x3, c.z);
-    x = x3;
-    if (e1) x = x1;
-    if (e2) x = x2;
-    y = sqrt_cand(g_of(x));
+// simplified SWU to E' (RFC 9380 section 6.6.2), then the 11-isogeny to E
+// (section 6.6.3): a Jacobian point, the identity when a denominator vanishes
+Jac<F> map_to_g1(const F& u) {
+    using namespace bls::h2c;
+    const F zu2 = mul(fconst(kZ), sqr(u));
+    const F tv1 = add(sqr(zu2), zu2);
+    const F x1 = is_zero(tv1) ? fconst(kSswuC2) : mul(fconst(kSswuC1), add(one(), inv(tv1)));
+    F x = x1;
+    if (!is_square(g_iso(x1))) x = mul(zu2, x1);
+    F y = sqrt_cand(g_iso(x));
     if (sgn0(u) != sgn0(y)) y = neg(y);
+    const F xn = horner(kIsoXNum, kIsoXNumLen, false, x), xd = horner(kIsoXDen, kIsoXDenLen, true, x);
+    const F yn = horner(kIsoYNum, kIsoYNumLen, false, x), yd = horner(kIsoYDen, kIsoYDenLen, true, x);
+    const F den = mul(xd, yd);
+    if (is_zero(den)) return Jac<F>{one(), one(), zero()};
+    const F di = inv(den);
+    return Jac<F>{mul(mul(xn, yd), di), mul(mul(mul(y, yn), xd), di), one()};
 }
 void hash_to_g1(const uint8_t* msg, size_t mlen, const uint8_t* dst, size_t dlen, uint64_t* out12) {
     uint8_t ub[128];
     expand_xmd(msg, mlen, dst, dlen, ub, 128);
     F u0 = field_from_64(ub), u1 = field_from_64(ub + 64);
-    F x0, y0, x1, y1;
-    map_svdw(u0, x0, y0);
-    map_svdw(u1, x1, y1);
-    Jac<F> q = addj(Jac<F>{x0, y0, one()}, Jac<F>{x1, y1, one()});
+    Jac<F> q = addj(map_to_g1(u0), map_to_g1(u1));
     const uint64_t heff[1] = {0xd201000000010001ULL};
     Jac<F> r = smul(q, heff, 1);
     F x, y;

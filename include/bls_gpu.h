@@ -301,10 +301,11 @@ int bls_verify_batch_rlc(bls_ctx* ctx, const bls_batch* batch, const uint64_t* s
 
 /* -H(m_i) for n messages on the GPU, in the neg_hms layout (12 x uint64 each,
  * affine Montgomery).  H is RFC 9380 hash_to_curve to G1 with
- * expand_message_xmd over SHA-256 and domain `dst` (0..255 bytes), using the
- * Shallue-van de Woestijne map (RFC 9380 section 6.6.1) and h_eff = 1 - x:
- * the RFC's SVDW suite.  ic_bls12_381's hash_to_curve uses the SSWU suite,
- * whose points differ, so callers that must match it keep hashing on the CPU.
+ * expand_message_xmd over SHA-256 and domain `dst` (0..255 bytes): the suite
+ * BLS12381G1_XMD:SHA-256_SSWU_RO_ (simplified SWU map on the 11-isogenous
+ * curve, the 11-isogeny to E, h_eff = 1 - x), the suite ic_bls12_381's
+ * hash_to_curve implements, so with the caller's domain string the points
+ * are the ones its CPU hash gives.
  * msgs: the messages back to back; offsets: n + 1 byte offsets, offsets[0] = 0,
  * non-decreasing (message i is msgs[offsets[i] .. offsets[i+1])). */
 int bls_neg_hash_to_g1(bls_ctx* ctx, const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst,

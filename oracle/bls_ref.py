@@ -22,7 +22,9 @@ mirrored by the reference's GPU code) for small cases:
     cuda/decompress.cu:140-188, performs none of them);
   * hash-to-G1 following RFC 9380's hash_to_curve construction
     (expand_message_xmd with SHA-256, hash_to_field, map_to_curve, clear_cofactor)
-    with the Shallue-van de Woestijne map of RFC 9380 section 6.6.1.
+    for the suite BLS12381G1_XMD:SHA-256_SSWU_RO_ that ic_bls12_381 implements:
+    the simplified SWU map of section 6.6.2 on the 11-isogenous curve E' and
+    the 11-isogeny to E, evaluated pointwise by Velu's formulas.
 
 Field elements are canonical Python ints in [0, p).  Montgomery limbs (R = 2^384,
 6 x u64 little-endian) are produced only at the boundary (`mont_limbs`).
@@ -791,7 +793,7 @@ def g1_from_mont_u64(limbs):
 
 
 # ----------------------------------------------------------------------------
-# Hash to G1: RFC 9380 hash_to_curve with the Shallue-van de Woestijne map
+# Hash to G1: RFC 9380 hash_to_curve, suite BLS12381G1_XMD:SHA-256_SSWU_RO_
 # ----------------------------------------------------------------------------
 
 def expand_message_xmd(msg, dst, len_in_bytes):
@@ -817,76 +819,198 @@ def hash_to_field_fp(msg, dst, count=2):
     return [int.from_bytes(ub[L * i:L * (i + 1)], "big") % P for i in range(count)]
 
 
-def _g(x):
-    return (x * x * x + B_G1) % P
-
-
-def _find_z_svdw():
-    """RFC 9380 appendix H.1 (A = 0, B = 4)."""
-    ctr = 1
-    while True:
-        for z in (ctr % P, (-ctr) % P):
-            gz = _g(z)
-            if gz == 0:
-                continue
-            h = (-(3 * z * z) * fp_inv(4 * gz % P)) % P
-            if h == 0 or not fp_is_square(h):
-                continue
-            if fp_is_square(gz) or fp_is_square(_g((-z) * fp_inv(2) % P)):
-                return z
-        ctr += 1
-
-
 def _sgn0(x):
     return x & 1
 
 
-SVDW_Z = _find_z_svdw()
-_gz = _g(SVDW_Z)
-SVDW_C1 = _gz
-SVDW_C2 = (-SVDW_Z) * fp_inv(2) % P
-_c3 = fp_sqrt((-_gz * (3 * SVDW_Z * SVDW_Z)) % P)
-assert _c3 * _c3 % P == (-_gz * (3 * SVDW_Z * SVDW_Z)) % P
-SVDW_C3 = _c3 if _sgn0(_c3) == 0 else (-_c3) % P
-SVDW_C4 = (-4 * _gz) * fp_inv(3 * SVDW_Z * SVDW_Z % P) % P
+# E': y^2 = x^3 + A' x + B', 11-isogenous to E (RFC 9380 section 8.8.1).  The
+# published coefficients are accepted because points of E' have orders that
+# divide #E(Fp) (tests/test_oracle.py checks it).
+SSWU_A = 0x144698a3b8e9433d693a02c96d4982b0ea985383ee66a8d8e8981aefd881ac98936f8da0e0f97f5cf428082d584c1d
+SSWU_B = 0x12e2908d11688030018b12e8753eee3b2016c1f0f24f4070a0b9c14fcef35ef55a23215a316ceaa5d1cc48e98e172be0
+# constant terms of the x and y numerators of the suite's isogeny map (RFC 9380
+# appendix E.2): they fix which of the six isomorphisms onto y^2 = x^3 + 4
+# the map uses
+ISO_X_NUM0 = 0x11a05f2b1e833340b809101dd99815856b303e88a2d7005ff2627b56cdb4e2c85610c2d5f2e62d6eaeac1662734649b7
+ISO_Y_NUM0 = 0x90d97c81ba24ee0259d1f094980dcfa11ad138e48a869522b52af6c956543d3cd0c7aee9b3ba3c2be9845719707bb33
+N_G1_CURVE = P + BLS_X                   # #E(Fp) = p + 1 - t, trace t = x + 1 = 1 - |x|
 
 
-def map_to_curve_svdw(u):
-    """RFC 9380 section 6.6.1, straight-line steps 1-36 (A = 0, B = 4)."""
-    tv1 = u * u % P
-    tv1 = tv1 * SVDW_C1 % P
-    tv2 = (1 + tv1) % P
-    tv1 = (1 - tv1) % P
-    tv3 = tv1 * tv2 % P
-    tv3 = fp_inv(tv3)
-    tv4 = u * tv1 % P
-    tv4 = tv4 * tv3 % P
-    tv4 = tv4 * SVDW_C3 % P
-    x1 = (SVDW_C2 - tv4) % P
-    gx1 = _g(x1)
-    e1 = fp_is_square(gx1)
-    x2 = (SVDW_C2 + tv4) % P
-    gx2 = _g(x2)
-    e2 = fp_is_square(gx2) and not e1
-    x3 = tv2 * tv2 % P
-    x3 = x3 * tv3 % P
-    x3 = x3 * x3 % P
-    x3 = x3 * SVDW_C4 % P
-    x3 = (x3 + SVDW_Z) % P
-    x = x3
-    if e1:
-        x = x1
-    if e2:
-        x = x2
-    gx = _g(x)
-    y = fp_sqrt(gx)
-    assert y * y % P == gx
+def _g_iso(x):
+    return (x * x * x + SSWU_A * x + SSWU_B) % P
+
+
+def _iso_add(a, b):
+    """affine addition on E' (None is the identity)"""
+    if a is None:
+        return b
+    if b is None:
+        return a
+    (x1, y1), (x2, y2) = a, b
+    if x1 == x2:
+        if (y1 + y2) % P == 0:
+            return None
+        lam = (3 * x1 * x1 + SSWU_A) * fp_inv(2 * y1 % P) % P
+    else:
+        lam = (y2 - y1) * fp_inv((x2 - x1) % P) % P
+    x3 = (lam * lam - x1 - x2) % P
+    return (x3, (lam * (x1 - x3) - y1) % P)
+
+
+def _iso_mul(a, k):
+    r = None
+    while k:
+        if k & 1:
+            r = _iso_add(r, a)
+        a = _iso_add(a, a)
+        k >>= 1
+    return r
+
+
+def _ptrim(a):
+    while a and a[-1] % P == 0:
+        a = a[:-1]
+    return a
+
+
+def _pmul(a, b):
+    r = [0] * (len(a) + len(b) - 1) if a and b else []
+    for i, x in enumerate(a):
+        for j, y in enumerate(b):
+            r[i + j] = (r[i + j] + x * y) % P
+    return _ptrim(r)
+
+
+def _prem(a, b):
+    """a mod b (coefficient lists, index = degree; b nonzero)"""
+    a, inv_lead = list(a), fp_inv(b[-1])
+    while len(a) >= len(b):
+        c, d = a[-1] * inv_lead % P, len(a) - len(b)
+        for i, y in enumerate(b):
+            a[d + i] = (a[d + i] - c * y) % P
+        a = _ptrim(a)
+    return a
+
+
+def _cubic_has_root(c0, c1):
+    """x^3 + c1 x + c0 has a root in Fp iff gcd(x^p - x, it) is not 1"""
+    cubic, xp, base, e = [c0 % P, c1 % P, 0, 1], [1], [0, 1], P
+    while e:
+        if e & 1:
+            xp = _prem(_pmul(xp, base), cubic)
+        base = _prem(_pmul(base, base), cubic)
+        e >>= 1
+    a, b = cubic, _ptrim([(xp[i] if i < len(xp) else 0) - (1 if i == 1 else 0) for i in range(3)])
+    b = [v % P for v in b]
+    while b:
+        a, b = b, _prem(a, b)
+    return len(a) > 1
+
+
+def _find_z_sswu():
+    """RFC 9380 appendix H.2: Z non-square, Z != -1, g(x) - Z irreducible,
+    g(B / (Z A)) square; smallest |Z| first, positive before negative."""
+    ctr = 1
+    while True:
+        for z in (ctr % P, (-ctr) % P):
+            if fp_is_square(z) or z == P - 1:
+                continue
+            if _cubic_has_root((SSWU_B - z) % P, SSWU_A):
+                continue
+            if not fp_is_square(_g_iso(SSWU_B * fp_inv(z * SSWU_A % P) % P)):
+                continue
+            return z
+        ctr += 1
+
+
+SSWU_Z = _find_z_sswu()
+
+
+def map_to_curve_sswu(u):
+    """RFC 9380 section 6.6.2 (the map's definition, steps 1-10) to E'."""
+    tv1 = (SSWU_Z * SSWU_Z * pow(u, 4, P) + SSWU_Z * u * u) % P
+    tv1 = fp_inv(tv1) if tv1 else 0
+    if tv1 == 0:
+        x1 = SSWU_B * fp_inv(SSWU_Z * SSWU_A % P) % P
+    else:
+        x1 = (-SSWU_B) * fp_inv(SSWU_A) % P * (1 + tv1) % P
+    gx1 = _g_iso(x1)
+    x2 = SSWU_Z * u * u % P * x1 % P
+    if fp_is_square(gx1):
+        x, y = x1, fp_sqrt(gx1)
+    else:
+        x, y = x2, fp_sqrt(_g_iso(x2))
     if _sgn0(u) != _sgn0(y):
         y = (-y) % P
     return (x, y)
 
 
+def _iso_kernel():
+    """the five points of a rational subgroup of order 11 of E', one of each
+    pair +-Q: (N / 11) times points of E' until the result is not O"""
+    x = 1
+    while True:
+        x += 1
+        if not fp_is_square(_g_iso(x)):
+            continue
+        q = _iso_mul((x, fp_sqrt(_g_iso(x))), N_G1_CURVE // 11)
+        if q is not None:
+            assert _iso_mul(q, 11) is None
+            out, acc = [], q
+            for _ in range(5):
+                out.append(acc)
+                acc = _iso_add(acc, q)
+            return out
+
+
+_ISO_KERNEL = _iso_kernel()
+
+
+def _velu(x):
+    """Velu's isogeny with the kernel above at abscissa x: (X(x), X'(x)), the
+    image being (X, y X'); None at a kernel abscissa"""
+    X, dX = x, 1
+    for xq, yq in _ISO_KERNEL:
+        h = (x - xq) % P
+        if h == 0:
+            return None
+        v = (6 * xq * xq + 2 * SSWU_A) % P
+        w = 4 * yq * yq % P
+        hi = fp_inv(h)
+        X = (X + v * hi + w * hi * hi) % P
+        dX = (dX - v * hi * hi - 2 * w * hi * hi % P * hi) % P
+    return X, dX
+
+
+def _iso_normalisation():
+    """(u^2, u^3) of the isomorphism onto y^2 = x^3 + 4, fixed by the suite's
+    two published coefficients: x_num(0) = u^2 X(0) D(0)^2 and
+    y_num(0) = u^3 X'(0) D(0)^3, D the kernel polynomial"""
+    d0 = 1
+    for xq, _ in _ISO_KERNEL:
+        d0 = d0 * (-xq) % P
+    X0, dX0 = _velu(0)
+    u2 = ISO_X_NUM0 * fp_inv(X0 * d0 * d0 % P) % P
+    u3 = ISO_Y_NUM0 * fp_inv(dX0 * pow(d0, 3, P) % P) % P
+    assert pow(u2, 3, P) == u3 * u3 % P, "the two coefficients give one isomorphism"
+    return u2, u3
+
+
+ISO_U2, ISO_U3 = _iso_normalisation()
+
+
+def iso_map(pt):
+    """E' -> E (affine; None for the identity)"""
+    if pt is None:
+        return None
+    x, y = pt
+    v = _velu(x)
+    if v is None:
+        return None
+    return (ISO_U2 * v[0] % P, ISO_U3 * y % P * v[1] % P)
+
+
 def hash_to_g1(msg, dst):
     u0, u1 = hash_to_field_fp(msg, dst, 2)
-    q = g1_add(map_to_curve_svdw(u0), map_to_curve_svdw(u1))
+    q = g1_add(iso_map(map_to_curve_sswu(u0)), iso_map(map_to_curve_sswu(u1)))
     return g1_mul(q, H_EFF_G1)

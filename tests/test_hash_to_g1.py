@@ -1,5 +1,6 @@
 """Hash to G1 on the GPU (bls_neg_hash_to_g1, bls_verify_messages): RFC 9380
-hash_to_curve with expand_message_xmd over SHA-256 and the SVDW map.  The
+hash_to_curve, suite BLS12381G1_XMD:SHA-256_SSWU_RO_ (ic_bls12_381's): the
+simplified SWU map on the 11-isogenous curve and the isogeny to E.  The
 reference's callers hash on the CPU (ic-integration/patches/
 ic-gpu-consensus.patch:454-457); the device constants are derived by
 icp-gpu_b200/csrc/gen_h2c.py and checked here against the oracle and hashlib,
@@ -50,8 +51,17 @@ def test_sha256_constants_against_hashlib():
 
 
 def test_map_constants_match_oracle():
-    assert H.SVDW_Z == B.SVDW_Z
-    assert (H.SVDW_C1, H.SVDW_C2, H.SVDW_C3, H.SVDW_C4) == (B.SVDW_C1, B.SVDW_C2, B.SVDW_C3, B.SVDW_C4)
+    assert H.SSWU_Z == B.SSWU_Z and (H.ISO_A, H.ISO_B) == (B.SSWU_A, B.SSWU_B)
+    assert H.SSWU_C1 == (-B.SSWU_B) * B.fp_inv(B.SSWU_A) % B.P
+    assert H.SSWU_C2 == B.SSWU_B * B.fp_inv(B.SSWU_Z * B.SSWU_A % B.P) % B.P
+    # the generator's rational map (kernel from the 11-division polynomial,
+    # Kohel's formulas) against the oracle's pointwise Velu map (kernel from a
+    # rational point of order 11): two derivations, one map
+    for u in (1, 99, 2**200 + 3, B.P - 5):
+        pt = B.map_to_curve_sswu(u)
+        assert H.iso_map(*pt) == B.iso_map(pt)
+    assert len(H.ISO_X_NUM) == 12 and len(H.ISO_Y_NUM) == 16
+    assert H.ISO_X_DEN[-1] == 1 and H.ISO_Y_DEN[-1] == 1 and len(H.ISO_X_DEN) == 11 and len(H.ISO_Y_DEN) == 16
     assert H.H_EFF == B.H_EFF_G1
     assert H.K256 == (1 << 256) * (1 << 768) % B.P
 
@@ -89,7 +99,7 @@ def test_hash_matches_oracle_lengths(ctx):
 @pytest.mark.gpu
 def test_hash_domains(ctx):
     msg = [b"abc"]
-    for dst in (b"X", b"QUUX-V01-CS02-with-BLS12381G1_XMD:SHA-256_SVDW_RO_", bytes(range(255))):
+    for dst in (b"X", b"BLS12381G1_XMD:SHA-256_SSWU_RO_TESTGEN", bytes(range(255))):
         assert (ctx.neg_hash_to_g1(msg, dst)[0] == _oracle_neg(msg[0], dst)).all()
 
 

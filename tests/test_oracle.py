@@ -180,12 +180,27 @@ def test_expand_message_xmd_shape_and_determinism():
     assert B.expand_message_xmd(b"abc", W.DST, 32) != a[:32]
 
 
-def test_svdw_constants_and_map():
-    z = B.SVDW_Z
-    assert z == B.P - 3       # first candidate of RFC 9380 appendix H.1 that passes
+def test_sswu_curve_z_and_map():
+    """E' is isogenous to E (its points have orders dividing #E(Fp) = h r), Z
+    is the RFC's search result, and the map lands on E' with sgn0(y) = sgn0(u)"""
+    assert B.N_G1_CURVE == 0x396c8c005555e1568c00aaab0000aaab * B.R_ORDER
+    x = 5
+    while not B.fp_is_square(B._g_iso(x)):
+        x += 1
+    assert B._iso_mul((x, B.fp_sqrt(B._g_iso(x))), B.N_G1_CURVE) is None
+    assert B.SSWU_Z == 11
     for u in (0, 1, 2, 12345, B.P - 1):
-        x, y = B.map_to_curve_svdw(u)
-        assert B.g1_on_curve((x, y)) and (y & 1) == (u & 1)
+        x, y = B.map_to_curve_sswu(u)
+        assert (y * y - B._g_iso(x)) % B.P == 0 and (y & 1) == (u & 1)
+
+
+def test_isogeny_lands_on_e_and_adds():
+    pts = [B.map_to_curve_sswu(u) for u in (3, 77, 2**300 + 5)]
+    imgs = [B.iso_map(q) for q in pts]
+    assert all(q is not None and B.g1_on_curve(q) for q in imgs)
+    assert B.iso_map(B._iso_add(pts[0], pts[1])) == B.g1_add(imgs[0], imgs[1])
+    assert B.iso_map(B._iso_mul(pts[2], 11)) == B.g1_mul(imgs[2], 11)
+    assert B.iso_map(B._ISO_KERNEL[0]) is None          # the kernel maps to the identity
 
 
 def test_hash_to_g1_in_subgroup():
