@@ -304,6 +304,8 @@ check_isogenous_curve()
 SSWU_Z = find_z_sswu()
 SSWU_C1 = (-ISO_B) * inv(ISO_A) % P                 # -B' / A'
 SSWU_C2 = ISO_B * inv(SSWU_Z * ISO_A % P) % P       # B' / (Z A'), x1 when tv1 = 0
+SQRT_RATIO_E = (P - 3) // 4                          # sqrt_ratio for p = 3 mod 4 (RFC 9380 F.2.1.2): c1
+SQRT_MINUS_Z = sqrt((-SSWU_Z) % P)                   # and c2 = sqrt(-Z) (any root: sgn0 fixes y)
 ISO_X_NUM, ISO_X_DEN, ISO_Y_NUM, ISO_Y_DEN = derive_isogeny()
 H_EFF = 1 - X_BLS
 K256 = (1 << 256) * R * R % P       # raw operand: mont_mul(hi, K256) = hi 2^256 R
@@ -339,8 +341,11 @@ def emit():
     arr("kSha256K", SHA256_K, "0x%08xu", "uint32_t")
     arr("kSha256H0", SHA256_H0, "0x%08xu", "uint32_t")
     L.append("// E': y^2 = x^3 + A' x + B', the SSWU map's Z, -B'/A' and B'/(Z A') (Montgomery)")
-    for name, v in (("kIsoA", ISO_A), ("kIsoB", ISO_B), ("kZ", SSWU_Z), ("kSswuC1", SSWU_C1), ("kSswuC2", SSWU_C2)):
+    for name, v in (("kIsoA", ISO_A), ("kIsoB", ISO_B), ("kZ", SSWU_Z), ("kSswuC1", SSWU_C1), ("kSswuC2", SSWU_C2),
+                    ("kSqrtMinusZ", SQRT_MINUS_Z)):
         fparr(name, [v])
+    arr("kSqrtRatioE", limbs64(SQRT_RATIO_E), "0x%016xull", "uint64_t")
+    L.append("constexpr int kSqrtRatioBits = %d;  // (p - 3) / 4" % SQRT_RATIO_E.bit_length())
     L.append("// the 11-isogeny E' -> E: coefficients by degree; the denominators are monic")
     L.append("// (leading 1 not stored): x = x_num / x_den, y = y' y_num / y_den")
     fparr("kIsoXNum", ISO_X_NUM)

@@ -136,47 +136,65 @@ __device__ __forceinline__ fp g_iso(const fp& x) {
     return fp_add(fp_mul(fp_add(fp_sqr(x), fp_load_u64(kIsoA)), x), fp_load_u64(kIsoB));
 }
 
-// the simplified SWU map to E', RFC 9380 section 6.6.2: x1 = (-B'/A')
-// (1 + 1 / (Z^2 u^4 + Z u^2)) (B' / (Z A') when that sum is 0), x2 = Z u^2 x1;
-// x1 when g'(x1) is a square, else x2 (then g'(x2) is one, by the choice of
-// Z); square roots by a^((p+1)/4), tested by squaring; sgn0(y) = sgn0(u)
-static __device__ __noinline__ void map_sswu(const fp& u, fp& x, fp& y) {
-    const fp zu2 = fp_mul(fp_load_u64(kZ), fp_sqr(u));
-    const fp tv1 = fp_add(fp_sqr(zu2), zu2);
-    fp x1;
-    if (fp_is_zero(tv1)) {
-        x1 = fp_load_u64(kSswuC2);
-    } else {
-        x1 = fp_mul(fp_load_u64(kSswuC1), fp_add(fp_one(), fp_inv0(tv1)));
-    }
-    const fp gx1 = g_iso(x1);
-    x = x1;
-    y = fp_sqrt_candidate(gx1);
-    if (!fp_eq(fp_sqr(y), gx1)) {
-        x = fp_mul(zu2, x1);
-        y = fp_sqrt_candidate(g_iso(x));
-    }
+// sqrt_ratio(u, v) for p = 3 mod 4 (RFC 9380 appendix F.2.1.2): true and
+// y = sqrt(u / v) when u / v is a square, else false and y = sqrt(Z u / v);
+// one exponentiation
+__device__ __forceinline__ bool sqrt_ratio(const fp& u, const fp& v, fp& y) {
+    const fp tv2 = fp_mul(u, v);
+    const fp tv1 = fp_mul(fp_sqr(v), tv2);                          // u v^3
+    const fp y1 = fp_mul(fp_pow_u64(tv1, kSqrtRatioE, kSqrtRatioBits), tv2);
+    const bool qr = fp_eq(fp_mul(fp_sqr(y1), v), u);
+    y = qr ? y1 : fp_mul(y1, fp_load_u64(kSqrtMinusZ));
+    return qr;
+}
+
+// the simplified SWU map to E' by the RFC's straight-line steps (appendix
+// F.2, steps 1-24), which give the map of section 6.6.2 with one
+// exponentiation: x' = xn / xd is returned as its two parts (the isogeny
+// takes a fraction), y' affine, sgn0(y') = sgn0(u)
+static __device__ __noinline__ void map_sswu(const fp& u, fp& xn, fp& xd, fp& y) {
+    const fp A = fp_load_u64(kIsoA), B = fp_load_u64(kIsoB), Z = fp_load_u64(kZ);
+    const fp tv1 = fp_mul(Z, fp_sqr(u));                            // Z u^2
+    const fp tv2 = fp_add(fp_sqr(tv1), tv1);                        // Z^2 u^4 + Z u^2
+    const fp tv3 = fp_mul(B, fp_add(tv2, fp_one()));
+    const fp tv4 = fp_mul(A, fp_is_zero(tv2) ? Z : fp_neg(tv2));    // x1 = tv3 / tv4
+    fp tv6 = fp_sqr(tv4);
+    const fp gn = fp_add(fp_mul(fp_add(fp_sqr(tv3), fp_mul(A, tv6)), tv3), fp_mul(B, fp_mul(tv6, tv4)));
+    tv6 = fp_mul(tv6, tv4);                                         // g'(x1) = gn / tv4^3
+    fp y1;
+    const bool sq = sqrt_ratio(gn, tv6, y1);
+    xn = sq ? tv3 : fp_mul(tv1, tv3);                               // x1 or x2 = Z u^2 x1
+    xd = tv4;
+    y = sq ? y1 : fp_mul(fp_mul(tv1, u), y1);
     if (sgn0(u) != sgn0(y)) y = fp_neg(y);
 }
 
-// c(x) by Horner over `len` coefficients of 6 u64 (Montgomery), plus x^len
-// when `monic`
-__device__ __forceinline__ fp horner(const uint64_t* c, int len, bool monic, const fp& x) {
-    fp acc = monic ? fp_one() : fp_load_u64(c + 6 * (len - 1));
-    for (int i = monic ? len - 1 : len - 2; i >= 0; --i) acc = fp_add(fp_mul(acc, x), fp_load_u64(c + 6 * i));
+// C(N, D) = D^deg c(N / D) for `len` coefficients of 6 u64 (Montgomery),
+// plus the leading 1 when `monic` (deg = len - 1 + monic): Horner in N with
+// the running power D^(deg - i) beside it
+__device__ __forceinline__ fp horner_h(const uint64_t* c, int len, bool monic, const fp& N, const fp& D) {
+    const int deg = len - 1 + (monic ? 1 : 0);
+    fp acc = monic ? fp_one() : fp_load_u64(c + 6 * (len - 1)), dk = D;
+    for (int i = deg - 1; i >= 0; --i) {
+        acc = fp_add(fp_mul(acc, N), fp_mul(fp_load_u64(c + 6 * i), dk));
+        dk = fp_mul(dk, D);
+    }
     return acc;
 }
 
 // the 11-isogeny E' -> E (RFC 9380 section 6.6.3 with the map of appendix
-// E.2), one inversion for both denominators; the Jacobian identity when a
-// denominator vanishes
-static __device__ __noinline__ g1j iso_map(const fp& xs, const fp& ys) {
-    const fp xn = horner(kIsoXNum, kIsoXNumLen, false, xs), xd = horner(kIsoXDen, kIsoXDenLen, true, xs);
-    const fp yn = horner(kIsoYNum, kIsoYNumLen, false, xs), yd = horner(kIsoYDen, kIsoYDenLen, true, xs);
-    const fp den = fp_mul(xd, yd);
-    if (fp_is_zero(den)) return {fp_one(), fp_one(), fp_zero()};
-    const fp di = fp_inv0(den);
-    return {fp_mul(fp_mul(xn, yd), di), fp_mul(fp_mul(fp_mul(ys, yn), xd), di), fp_one()};
+// E.2) at x' = N / D, straight to Jacobian coordinates without an inversion:
+// x = x_num / x_den = XN / (XD D), y = y' YN / YD (the powers of D cancel),
+// Z = x_den y_den, X = x_num x_den y_den^2, Y = y_num x_den^3 y_den^2.  A
+// vanishing denominator gives Z = 0, the identity.
+static __device__ __noinline__ g1j iso_map(const fp& N, const fp& D, const fp& ys) {
+    const fp xnum = horner_h(kIsoXNum, kIsoXNumLen, false, N, D);                  // D^11 x_num(x')
+    const fp xden = fp_mul(horner_h(kIsoXDen, kIsoXDenLen, true, N, D), D);        // D^11 x_den(x')
+    const fp ynum = fp_mul(ys, horner_h(kIsoYNum, kIsoYNumLen, false, N, D));      // D^15 y' y_num(x')
+    const fp yden = horner_h(kIsoYDen, kIsoYDenLen, true, N, D);                   // D^15 y_den(x')
+    const fp yd2 = fp_sqr(yden);
+    return {fp_mul(fp_mul(xnum, xden), yd2), fp_mul(fp_mul(ynum, fp_mul(fp_sqr(xden), xden)), yd2),
+            fp_mul(xden, yden)};
 }
 
 // affine (x, y) of a Jacobian point; false for the identity

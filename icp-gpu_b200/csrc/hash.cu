@@ -26,9 +26,9 @@ __global__ void __launch_bounds__(kHashThreads) k_neg_hash_to_g1(const uint8_t* 
         const uint32_t a = offsets[i], b = offsets[i + 1];
         uint32_t ub[32];
         h2c::expand_xmd_128(msgs + a, b - a, dst, (uint32_t)dst_len, ub);
-        fp xs, ys;
-        h2c::map_sswu(h2c::field_from_be64(ub + 16 * which), xs, ys);
-        pt = h2c::iso_map(xs, ys);
+        fp xn, xd, ys;
+        h2c::map_sswu(h2c::field_from_be64(ub + 16 * which), xn, xd, ys);
+        pt = h2c::iso_map(xn, xd, ys);
         if (which) {
             uint4* d = xch[threadIdx.x >> 1];
             const fp* c[3] = {&pt.X, &pt.Y, &pt.Z};
