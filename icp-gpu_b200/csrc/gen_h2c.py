@@ -353,7 +353,7 @@ def emit():
     fparr("kIsoYNum", ISO_Y_NUM)
     fparr("kIsoYDen", ISO_Y_DEN[:-1])
     arr("kK256", limbs64(K256), "0x%016xull", "uint64_t")
-    arr("kPMinus2", limbs64(P - 2), "0x%016xull", "uint64_t")
+    arr("kR3", [(R ** 3 % P >> (32 * i)) & 0xffffffff for i in range(12)], "0x%08xu", "uint32_t")
     L.append("constexpr uint64_t kHEff = 0x%016xull;  // 1 - x" % H_EFF)
     L.append("constexpr int kIsoXNumLen = %d, kIsoXDenLen = %d, kIsoYNumLen = %d, kIsoYDenLen = %d;"
              % (len(ISO_X_NUM), len(ISO_X_DEN) - 1, len(ISO_Y_NUM), len(ISO_Y_DEN) - 1))

@@ -9,6 +9,7 @@
 // which derives the isogeny; the kernel (hash.cu) runs the two maps of a
 // message on two threads.
 #pragma once
+#include "fp_inv.cuh"
 #include "g1.cuh"
 #include "h2c.inc"
 
@@ -125,10 +126,6 @@ __device__ __forceinline__ fp field_from_be64(const uint32_t* w) {
     return fp_add(fp_mul(lo, fp_rr()), fp_mul(hi, fp_load_u64(kK256)));
 }
 
-static __device__ __noinline__ fp fp_inv0(const fp& a) {   // 0 for 0 (RFC 9380 inv0)
-    return fp_pow_u64(a, kPMinus2, 381);
-}
-
 __device__ __forceinline__ uint32_t sgn0(const fp& a) { return fp_from_mont(a).w[0] & 1u; }
 
 // g'(x) = x^3 + A' x + B' on E'
@@ -200,7 +197,7 @@ static __device__ __noinline__ g1j iso_map(const fp& N, const fp& D, const fp& y
 // affine (x, y) of a Jacobian point; false for the identity
 __device__ __forceinline__ bool to_affine(const g1j& p, fp& x, fp& y) {
     if (fp_is_zero(p.Z)) return false;
-    const fp zi = fp_inv0(p.Z), zi2 = fp_sqr(zi);
+    const fp zi = fp_inverse_mont(p.Z, kR3), zi2 = fp_sqr(zi);
     x = fp_mul(p.X, zi2);
     y = fp_mul(p.Y, fp_mul(zi2, zi));
     return true;

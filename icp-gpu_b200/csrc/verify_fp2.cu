@@ -227,7 +227,7 @@ __device__ __forceinline__ void finish(uint32_t off, const uint32_t* sm, const B
         if (half == 0) {
             fp z;
             load_fp(z.w, sm, slot_addr(bs, lin[0] >> 8), 0);
-            fp r = f2::fp_inverse_mont(z);
+            fp r = fp_inverse_mont(z, f2::kR3);
 #pragma unroll
             for (int i = 0; i < 12; ++i) o[i] = r.w[i];
         } else {
