@@ -309,14 +309,15 @@ def run_gpu(args):
     e2e_value = whole_job_rate(N_ITEMS, world, args.steps, e2e_s)
 
     chain_timad = ctx.imad_chain_rate() / 1e12
-    batching = serving = ingest = hashing = rlc = None
-    # the single-GPU sections (ingest, hashing, random linear combinations,
-    # batching, serving) run on one GPU only; under torchrun every rank times
+    batching = serving = ingest = hashing = rlc = compressed = None
+    # the single-GPU sections (ingest, hashing, compressed signatures, random
+    # linear combinations, batching, serving) run on one GPU only; under torchrun every rank times
     # the headline step alone
     if not args.no_extras and world == 1:
         sizes = [int(v) for v in args.ingest_keys.split(",") if int(v) > 0]
         ingest = [run_ingest(G, WL, local, args.lanes, k) for k in sizes] or None
         hashing = run_hash(G, WL, ctx, wl, pk_ids)
+        compressed = run_compressed(G, WL, ctx, n=args.compressed_items) if args.compressed_items > 0 else None
         rlc = run_rlc(G, WL, ctx, wl, pk_ids, n=args.rlc_items) if args.rlc_items > 0 else None
         batching = run_batching(G, WL, ctx, ids)
         if args.serve_seconds > 0:
@@ -369,6 +370,8 @@ def run_gpu(args):
             result["ingest"] = ingest
         if hashing:
             result["hash"] = hashing
+        if compressed:
+            result["compressed"] = compressed
         if rlc:
             result["rlc"] = rlc
         if batching:
@@ -383,6 +386,63 @@ def run_gpu(args):
         pg.destroy_process_group()
     if result is not None:
         print(json.dumps(result), flush=True)
+
+
+def run_compressed(G, WL, ctx, n=65536, reps=3):
+    """Compressed workload: n 48-byte signatures over 40 keys, 2% of them
+    invalid encodings (bad flags, x >= p, off the curve, outside the subgroup)
+    with the reason per index known.  Decode, checks and verify in one launch
+    (bls_verify_batch with BLS_SIG_COMPRESSED) from host buffers, and the same
+    through two calls (bls_g1_decompress_status, then the affine verify of the
+    decoded points, statuses merged: the reference's decompress-then-verify
+    flow, ic-integration/gpu_crypto/lib.rs:189-223 then :124-160).  Host-timed,
+    best of reps; every result checked against the known one."""
+    import torch
+    wl = WL.config_compressed(n, 40, seed=3)
+    ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)[wl["pk_index"]]
+    enc = wl["sigs_compressed"]
+    expect = wl["expect"]
+
+    def fused():
+        return ctx.verify(enc, wl["nhms"], ids, compressed=True)
+
+    def two_calls():
+        st, xy = ctx.g1_decompress(enc.tobytes())
+        r = ctx.verify(xy, wl["nhms"], ids)
+        return np.where(st != 0, -st, r)
+
+    out = {"items": n, "keys": 40, "invalid": int((expect < 0).sum()),
+           "api": "bls_verify_batch, BLS_SIG_COMPRESSED (host buffers): decode, checks and verify in one launch"}
+    for name, fn in (("fused", fused), ("decompress_then_verify", two_calls)):
+        assert (fn() == expect).all(), name + ": results differ from the expected ones"
+        best = 1e30
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            best = min(best, time.perf_counter() - t0)
+        out[name + "_verifies_per_s"] = round(n / best, 1)
+    # the fused launch alone, inputs resident (CUDA events on the library's stream)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_enc = torch.from_numpy(np.ascontiguousarray(enc).reshape(-1)).to(dev)
+    d_nhms = torch.from_numpy(wl["nhms"].view(np.int64)).to(dev)
+    d_ids = torch.from_numpy(ids).to(dev)
+    d_res = torch.zeros(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    times = []
+    for k in range(reps + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            ctx.verify_device(n, d_enc.data_ptr(), d_nhms.data_ptr(), d_ids.data_ptr(), d_res.data_ptr(),
+                              compressed=True)
+            b.record(stream)
+        ctx.sync()
+        if k:
+            times.append(a.elapsed_time(b))
+    assert (d_res.cpu().numpy() == expect).all(), "device-resident compressed verify differs"
+    out["kernel_ms"] = round(min(times), 3)
+    out["verifies_per_s"] = round(n / (min(times) / 1e3), 1)
+    return out
 
 
 def run_batching(G, WL, ctx, ids_unused, reps=2):
@@ -599,6 +659,8 @@ def main():
     ap.add_argument("--ingest-keys", default="1024,16384",
                     help="comma-separated key counts ingested compressed on the GPU (0 = skip)")
     ap.add_argument("--rlc-items", type=int, default=65536, help="random-linear-combination batch draw (0 = skip)")
+    ap.add_argument("--compressed-items", type=int, default=65536,
+                    help="compressed workload: 48-byte signatures, 2%% invalid encodings (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the serving stream (0 = skip)")
     ap.add_argument("--serve-mode", choices=["ring", "slots"], default="ring", help="serving: server mode")
     ap.add_argument("--serve-ring-blocks", type=int, default=4,
