@@ -10,6 +10,7 @@
 // whatever order the device evaluates the same formula in.
 #pragma once
 #include "fp.cuh"
+#include "fp_inv.cuh"
 
 namespace bls {
 
@@ -45,11 +46,11 @@ static __device__ __noinline__ fp2 fp2_sqr(const fp2& a) {
     return {s, fp_add(t, t)};
 }
 
-// Fermat a^(p-2) (field_sppark.cuh:40-50); maps 0 to 0
+// a^-1, 0 for 0 (the reference's Fermat a^(p-2), field_sppark.cuh:40-50,
+// gives the same value): the binary extended Euclid of fp_inv.cuh
 static __device__ __noinline__ fp fp_inv(const fp& a) {
-    const uint64_t e[6] = {0xb9feffffffffaaa9ULL, 0x1eabfffeb153ffffULL, 0x6730d2a0f6b0f624ULL,
-                           0x64774b84f38512bfULL, 0x4b1ba7b6434bacd7ULL, 0x1a0111ea397fe69aULL};
-    return fp_pow_u64(a, e, 381);
+    const fp r3 = fp_mul(fp_rr(), fp_rr());              // R^3 mod p
+    return fp_inverse_mont(a, r3.w);
 }
 static __device__ __noinline__ fp2 fp2_inv(const fp2& a) {
     fp n = fp_add(fp_sqr(a.c0), fp_sqr(a.c1));
