@@ -1,0 +1,51 @@
+"""Batches far larger than one wave of the verify kernel (888 resident blocks of
+five verifications on a B200), with ragged sizes: every result against the
+workload's known answer, and the same items verified in one call and in
+uneven chunks give the same results."""
+import numpy as np
+import pytest
+
+import bls_gpu as G
+import workload_py as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    G.init()
+    with G.Context(lanes=6) as c:
+        yield c
+
+
+@pytest.fixture(scope="module")
+def big():
+    return W.WL.config_keyset(40003, 40, seed=41)
+
+
+def _ids(ctx, wl):
+    ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
+    return ids[wl["pk_index"]]
+
+
+def test_multi_wave_batch_is_exact(ctx, big):
+    ids = _ids(ctx, big)
+    res = ctx.verify(big["sigs"], big["nhms"], ids)
+    assert (res == big["expect"]).all()
+    assert (big["expect"] == 0).sum() > 4000          # 1 in 8 corrupted, both kinds
+
+
+def test_chunked_equals_one_call(ctx, big):
+    ids = _ids(ctx, big)
+    whole = ctx.verify(big["sigs"], big["nhms"], ids)
+    cuts = [0, 1, 6, 4099, 17000, 33333, len(ids)]
+    parts = [ctx.verify(big["sigs"][a:b], big["nhms"][a:b], ids[a:b]) for a, b in zip(cuts, cuts[1:])]
+    assert (np.concatenate(parts) == whole).all()
+
+
+def test_compressed_multi_wave_with_invalid(ctx):
+    wl = W.WL.config_compressed(n=20011, nkeys=40, seed=43)
+    ids = _ids(ctx, wl)
+    res = ctx.verify(wl["sigs_compressed"], wl["nhms"], ids, compressed=True)
+    assert (res == wl["expect"]).all()
+    assert (wl["expect"] < 0).sum() == round(0.02 * 20011)
