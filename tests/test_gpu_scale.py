@@ -1,7 +1,11 @@
 """Batches far larger than one wave of the verify kernel (888 resident blocks of
 five verifications on a B200), with ragged sizes: every result against the
 workload's known answer, and the same items verified in one call and in
-uneven chunks give the same results."""
+uneven chunks give the same results.  And concurrent callers: the reference
+ABI and one shared context called from several host threads at once (the
+reference's library is not thread-safe; this one's entry points are)."""
+import threading
+
 import numpy as np
 import pytest
 
@@ -49,3 +53,42 @@ def test_compressed_multi_wave_with_invalid(ctx):
     res = ctx.verify(wl["sigs_compressed"], wl["nhms"], ids, compressed=True)
     assert (res == wl["expect"]).all()
     assert (wl["expect"] < 0).sum() == round(0.02 * 20011)
+
+
+def _run_threads(fn, n):
+    errors = []
+
+    def body(k):
+        try:
+            fn(k)
+        except Exception as e:          # noqa: BLE001 - reported below
+            errors.append(repr(e))
+    th = [threading.Thread(target=body, args=(k,)) for k in range(n)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors, errors
+
+
+def test_reference_abi_concurrent_callers(golden):
+    wls = [W.plain_config(n=24 + 7 * k, seed=60 + k) for k in range(4)]
+
+    def call(k):
+        wl = wls[k]
+        for _ in range(3):
+            got = G.batch_bls_verify(wl["sigs"], wl["nhms"], golden["g2_gen_coeffs"], wl["pk_tabs"])
+            assert [int(x) for x in got] == list(wl["expect"])
+    _run_threads(call, 4)
+
+
+def test_shared_context_concurrent_callers(ctx, big):
+    ids = _ids(ctx, big)
+    cuts = [0, 5000, 9001, 16384, 20000]
+
+    def call(k):
+        a, b = cuts[k], cuts[k + 1]
+        for _ in range(2):
+            r = ctx.verify(big["sigs"][a:b], big["nhms"][a:b], ids[a:b])
+            assert (r == big["expect"][a:b]).all()
+    _run_threads(call, 4)
