@@ -308,6 +308,29 @@ def run_gpu(args):
     e2e_s = max_over_ranks(pg, sum(e2e_times), dev)
     e2e_value = whole_job_rate(N_ITEMS, world, args.steps, e2e_s)
 
+    # the same items through the reference's own entry point, unchanged callers'
+    # view: per-item line tables from host memory (19,584 B each), no resident
+    # keys.  That entry point uses device 0, as the reference's does, so only a
+    # one-GPU run times it.
+    ref_abi = None
+    if world == 1:
+        item_tables = np.ascontiguousarray(wl["pk_tables"][wl["pk_index"]])
+        g2_table = generator_table(WL)
+        ref_abi_times = []
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            r = G.batch_bls_verify(wl["sigs"], wl["nhms"], g2_table, item_tables)
+            dt = time.perf_counter() - t0
+            if k >= args.warmup:
+                ref_abi_times.append(dt)
+        assert [int(x) for x in r] == list(wl["expect"])
+        ref_abi = {"value": round(N_ITEMS * args.steps / sum(ref_abi_times), 1), "unit": "verifies/s",
+                   "api": "gpu_batch_bls_verify (the reference's entry point: per-item line tables from host "
+                          "buffers, no resident keys)",
+                   "h2d_bytes_per_step": int(wl["sigs"].nbytes + wl["nhms"].nbytes + item_tables.nbytes
+                                             + g2_table.nbytes),
+                   "d2h_bytes_per_step": int(N_ITEMS * 4)}
+
     chain_timad = ctx.imad_chain_rate() / 1e12
     batching = serving = ingest = hashing = rlc = compressed = None
     # the single-GPU sections (ingest, hashing, compressed signatures, random
@@ -366,6 +389,8 @@ def run_gpu(args):
             "gpu_launches": args.steps,
             "bit_exact": True,
         }
+        if ref_abi:
+            result["e2e"]["reference_abi"] = ref_abi
         if ingest:
             result["ingest"] = ingest
         if hashing:

@@ -20,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <sys/random.h>
@@ -153,6 +154,60 @@ struct bls_ctx {
         b.cap = want;
         return BLS_OK;
     }
+
+    // Large host inputs (the reference entry point's per-item line tables,
+    // 19,584 B an item) copy from pageable memory at a fraction of the link's
+    // rate, so they go through two pinned staging buffers in turn: a team of
+    // host threads fills one round's buffer, each thread enqueueing the DMA of
+    // its share as soon as its memcpy is done, while the previous round's DMAs
+    // run.  Ordered on `stream` like a plain cudaMemcpyAsync.
+    static constexpr size_t kStageBytes = size_t(32) << 20;
+    HostBuf h_stage[2];
+    cudaEvent_t ev_stage[2] = {nullptr, nullptr};
+    int stage_h2d(void* dst, const void* src, size_t bytes) {
+        if (bytes < (size_t(4) << 20)) {
+            CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+            return BLS_OK;
+        }
+        for (int b = 0; b < 2; ++b) {
+            int rc = grow(h_stage[b], kStageBytes);
+            if (rc) return rc;
+            if (!ev_stage[b]) CK(cudaEventCreateWithFlags(&ev_stage[b], cudaEventDisableTiming));
+        }
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int nt = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+        const int dev = cfg.device;
+        for (size_t off = 0, round = 0; off < bytes; off += kStageBytes, ++round) {
+            const size_t len = std::min(kStageBytes, bytes - off);
+            const int b = (int)(round & 1);
+            CK(cudaEventSynchronize(ev_stage[b]));   // the DMAs that last read this buffer are done
+            char* stage = (char*)h_stage[b].p;
+            const size_t piece = (len + nt - 1) / nt;
+            std::vector<cudaError_t> err((size_t)nt, cudaSuccess);
+            auto work = [&](int t) {
+                const size_t a = std::min(len, piece * t), e = std::min(len, a + piece);
+                if (a >= e) return;
+                memcpy(stage + a, (const char*)src + off + a, e - a);
+                err[t] = cudaSetDevice(dev);
+                if (err[t] == cudaSuccess)
+                    err[t] = cudaMemcpyAsync((char*)dst + off + a, stage + a, e - a, cudaMemcpyHostToDevice, stream);
+            };
+            std::vector<std::thread> team;
+            for (int t = 1; t < nt; ++t) {
+                try {
+                    team.emplace_back(work, t);
+                } catch (...) {
+                    work(t);   // no thread to be had: this thread copies that share too
+                }
+            }
+            work(0);
+            for (auto& th : team) th.join();
+            for (cudaError_t e : err) CK(e);
+            CK(cudaEventRecord(ev_stage[b], stream));
+        }
+        return BLS_OK;
+    }
+
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -163,8 +218,10 @@ struct bls_ctx {
         for (DevBuf* b : {&d_sigs, &d_nhms, &d_pkidx, &d_res, &d_ml, &d_gt, &d_pk_items, &d_g2_call, &d_in,
                           &d_xy, &d_st, &d_work, &d_msg, &d_off, &d_dst, &d_rlc})
             if (b->p) cudaFree(b->p);
-        for (HostBuf* b : {&h_sigs, &h_nhms, &h_pkidx, &h_res})
+        for (HostBuf* b : {&h_sigs, &h_nhms, &h_pkidx, &h_res, &h_stage[0], &h_stage[1]})
             if (b->p) cudaFreeHost(b->p);
+        for (cudaEvent_t e : ev_stage)
+            if (e) cudaEventDestroy(e);
         if (d_g2) cudaFree(d_g2);
         if (d_pk) cudaFree(d_pk);
         if (d_pk_inf) cudaFree(d_pk_inf);
@@ -950,7 +1007,7 @@ int gpu_batch_bls_verify(const uint64_t* sigs, const uint64_t* neg_hms, const ui
         CK(cudaMemcpyAsync(c->d_sigs.p, sigs, n * 96, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->d_nhms.p, neg_hms, n * 96, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->d_g2_call.p, g2_coeffs, bls::kCoeffU64 * 8, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->d_pk_items.p, pk_coeffs, n * bls::kCoeffU64 * 8, cudaMemcpyHostToDevice, c->stream));
+        if ((rc = c->stage_h2d(c->d_pk_items.p, pk_coeffs, n * bls::kCoeffU64 * 8))) return rc;
         bls::VerifyArgs a{};
         a.sigs = c->d_sigs.p;
         a.sig_compressed = 0;
