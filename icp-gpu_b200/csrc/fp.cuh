@@ -338,4 +338,18 @@ __device__ __forceinline__ fp fp_pow_u64(const fp& a, const uint64_t* e, int nbi
     return r;
 }
 
+// An out-of-line Montgomery multiply, and a power over it, for code that runs
+// few warps per scheduler (a thread per point, per key or per message): there
+// nothing hides a miss in the instruction cache, and a loop that inlines a
+// multiply of several hundred instructions at every use misses on each pass.
+static __device__ __noinline__ fp fp_mul_ool(const fp& a, const fp& b) { return fp_mul(a, b); }
+__device__ __forceinline__ fp fp_pow_ool(const fp& a, const uint64_t* e, int nbits) {
+    fp r = fp_one(), base = a;
+    for (int i = 0; i < nbits; ++i) {
+        if ((e[i >> 6] >> (i & 63)) & 1) r = fp_mul_ool(r, base);
+        base = fp_mul_ool(base, base);
+    }
+    return r;
+}
+
 }  // namespace bls

@@ -32,7 +32,7 @@ __device__ __forceinline__ fp fp_four() {
 static __device__ __noinline__ fp fp_sqrt_candidate(const fp& a) {
     const uint64_t e[6] = {0xee7fbfffffffeaabULL, 0x07aaffffac54ffffULL, 0xd9cc34a83dac3d89ULL,
                            0xd91dd2e13ce144afULL, 0x92c6e9ed90d2eb35ULL, 0x0680447a8e5ff9a6ULL};
-    return fp_pow_u64(a, e, 379);
+    return fp_pow_ool(a, e, 379);
 }
 
 // canonical value > (p - 1) / 2
@@ -53,29 +53,33 @@ __device__ __forceinline__ bool fp_lex_largest(const fp& a) {
 // Jacobian coordinates on y^2 = x^3 + 4
 struct g1j { fp X, Y, Z; };
 
+// The Jacobian routines run one thread per point, a few warps per scheduler:
+// their products are the out-of-line multiply of fp.cuh.
+__device__ __forceinline__ fp fp_sqr_ool(const fp& a) { return fp_mul_ool(a, a); }
+
 // dbl-2009-l (a = 0)
 static __device__ __noinline__ g1j g1j_dbl(const g1j& p) {
-    fp A = fp_sqr(p.X), B = fp_sqr(p.Y), C = fp_sqr(B);
-    fp D = fp_sub(fp_sub(fp_sqr(fp_add(p.X, B)), A), C);
+    fp A = fp_sqr_ool(p.X), B = fp_sqr_ool(p.Y), C = fp_sqr_ool(B);
+    fp D = fp_sub(fp_sub(fp_sqr_ool(fp_add(p.X, B)), A), C);
     D = fp_add(D, D);
     fp E = fp_add(fp_add(A, A), A);
-    fp F = fp_sqr(E);
+    fp F = fp_sqr_ool(E);
     g1j r;
     r.X = fp_sub(F, fp_add(D, D));
     fp C8 = fp_add(C, C);
     C8 = fp_add(C8, C8);
     C8 = fp_add(C8, C8);
-    r.Y = fp_sub(fp_mul(E, fp_sub(D, r.X)), C8);
-    r.Z = fp_mul(fp_add(p.Y, p.Y), p.Z);
+    r.Y = fp_sub(fp_mul_ool(E, fp_sub(D, r.X)), C8);
+    r.Z = fp_mul_ool(fp_add(p.Y, p.Y), p.Z);
     return r;
 }
 
 // p + (qx, qy) with q affine (madd-2007-bl), exceptional cases handled
 static __device__ __noinline__ g1j g1j_add_affine(const g1j& p, const fp& qx, const fp& qy) {
     if (fp_is_zero(p.Z)) return {qx, qy, fp_one()};
-    fp Z1Z1 = fp_sqr(p.Z);
-    fp U2 = fp_mul(qx, Z1Z1);
-    fp S2 = fp_mul(fp_mul(qy, p.Z), Z1Z1);
+    fp Z1Z1 = fp_sqr_ool(p.Z);
+    fp U2 = fp_mul_ool(qx, Z1Z1);
+    fp S2 = fp_mul_ool(fp_mul_ool(qy, p.Z), Z1Z1);
     fp H = fp_sub(U2, p.X);
     fp rr = fp_sub(S2, p.Y);
     if (fp_is_zero(H)) {
@@ -83,16 +87,16 @@ static __device__ __noinline__ g1j g1j_add_affine(const g1j& p, const fp& qx, co
         return {fp_one(), fp_one(), fp_zero()};
     }
     rr = fp_add(rr, rr);
-    fp HH = fp_sqr(H);
+    fp HH = fp_sqr_ool(H);
     fp I = fp_add(HH, HH);
     I = fp_add(I, I);
-    fp J = fp_mul(H, I);
-    fp V = fp_mul(p.X, I);
+    fp J = fp_mul_ool(H, I);
+    fp V = fp_mul_ool(p.X, I);
     g1j r;
-    r.X = fp_sub(fp_sub(fp_sqr(rr), J), fp_add(V, V));
-    fp YJ = fp_mul(p.Y, J);
-    r.Y = fp_sub(fp_mul(rr, fp_sub(V, r.X)), fp_add(YJ, YJ));
-    r.Z = fp_sub(fp_sub(fp_sqr(fp_add(p.Z, H)), Z1Z1), HH);
+    r.X = fp_sub(fp_sub(fp_sqr_ool(rr), J), fp_add(V, V));
+    fp YJ = fp_mul_ool(p.Y, J);
+    r.Y = fp_sub(fp_mul_ool(rr, fp_sub(V, r.X)), fp_add(YJ, YJ));
+    r.Z = fp_sub(fp_sub(fp_sqr_ool(fp_add(p.Z, H)), Z1Z1), HH);
     return r;
 }
 
@@ -100,9 +104,9 @@ static __device__ __noinline__ g1j g1j_add_affine(const g1j& p, const fp& qx, co
 static __device__ __noinline__ g1j g1j_add(const g1j& p, const g1j& q) {
     if (fp_is_zero(p.Z)) return q;
     if (fp_is_zero(q.Z)) return p;
-    const fp Z1Z1 = fp_sqr(p.Z), Z2Z2 = fp_sqr(q.Z);
-    const fp U1 = fp_mul(p.X, Z2Z2), U2 = fp_mul(q.X, Z1Z1);
-    const fp S1 = fp_mul(fp_mul(p.Y, q.Z), Z2Z2), S2 = fp_mul(fp_mul(q.Y, p.Z), Z1Z1);
+    const fp Z1Z1 = fp_sqr_ool(p.Z), Z2Z2 = fp_sqr_ool(q.Z);
+    const fp U1 = fp_mul_ool(p.X, Z2Z2), U2 = fp_mul_ool(q.X, Z1Z1);
+    const fp S1 = fp_mul_ool(fp_mul_ool(p.Y, q.Z), Z2Z2), S2 = fp_mul_ool(fp_mul_ool(q.Y, p.Z), Z1Z1);
     const fp H = fp_sub(U2, U1);
     fp rr = fp_sub(S2, S1);
     if (fp_is_zero(H)) {
@@ -110,15 +114,15 @@ static __device__ __noinline__ g1j g1j_add(const g1j& p, const g1j& q) {
         return {fp_one(), fp_one(), fp_zero()};
     }
     fp I = fp_add(H, H);
-    I = fp_sqr(I);
-    const fp J = fp_mul(H, I);
+    I = fp_sqr_ool(I);
+    const fp J = fp_mul_ool(H, I);
     rr = fp_add(rr, rr);
-    const fp V = fp_mul(U1, I);
+    const fp V = fp_mul_ool(U1, I);
     g1j r;
-    r.X = fp_sub(fp_sub(fp_sqr(rr), J), fp_add(V, V));
-    const fp SJ = fp_mul(S1, J);
-    r.Y = fp_sub(fp_mul(rr, fp_sub(V, r.X)), fp_add(SJ, SJ));
-    r.Z = fp_mul(fp_sub(fp_sub(fp_sqr(fp_add(p.Z, q.Z)), Z1Z1), Z2Z2), H);
+    r.X = fp_sub(fp_sub(fp_sqr_ool(rr), J), fp_add(V, V));
+    const fp SJ = fp_mul_ool(S1, J);
+    r.Y = fp_sub(fp_mul_ool(rr, fp_sub(V, r.X)), fp_add(SJ, SJ));
+    r.Z = fp_mul_ool(fp_sub(fp_sub(fp_sqr_ool(fp_add(p.Z, q.Z)), Z1Z1), Z2Z2), H);
     return r;
 }
 

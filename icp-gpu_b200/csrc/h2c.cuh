@@ -130,38 +130,8 @@ __device__ __forceinline__ uint32_t sgn0(const fp& a) { return fp_from_mont(a).w
 
 // The hash kernel runs one warp per scheduler, so nothing hides a miss in the
 // instruction cache: its long loops (the sqrt_ratio power, the isogeny's
-// Horner evaluations, the 63 doublings of the cofactor clearing) call one
-// out-of-line Montgomery multiply and square instead of inlining a body of
-// several hundred instructions at every use.
-static __device__ __noinline__ fp hmul(const fp& a, const fp& b) { return fp_mul(a, b); }
-static __device__ __noinline__ fp hsqr(const fp& a) { return fp_sqr(a); }
-
-// a^e for an exponent of nbits bits (6 x u64, least significant bit first)
-__device__ __forceinline__ fp hpow(const fp& a, const uint64_t* e, int nbits) {
-    fp r = fp_one(), base = a;
-    for (int i = 0; i < nbits; ++i) {
-        if ((e[i >> 6] >> (i & 63)) & 1) r = hmul(r, base);
-        base = hsqr(base);
-    }
-    return r;
-}
-
-// the doubling of g1.cuh (dbl-2009-l, a = 0) on the out-of-line products
-static __device__ __noinline__ g1j hdbl(const g1j& p) {
-    const fp A = hsqr(p.X), B = hsqr(p.Y), C = hsqr(B);
-    fp D = fp_sub(fp_sub(hsqr(fp_add(p.X, B)), A), C);
-    D = fp_add(D, D);
-    const fp E = fp_add(fp_add(A, A), A);
-    const fp F = hsqr(E);
-    g1j r;
-    r.X = fp_sub(F, fp_add(D, D));
-    fp C8 = fp_add(C, C);
-    C8 = fp_add(C8, C8);
-    C8 = fp_add(C8, C8);
-    r.Y = fp_sub(hmul(E, fp_sub(D, r.X)), C8);
-    r.Z = hmul(fp_add(p.Y, p.Y), p.Z);
-    return r;
-}
+// Horner evaluations, the 63 doublings of the cofactor clearing) use the
+// out-of-line multiply of fp.cuh rather than inlining its body at every use.
 
 // g'(x) = x^3 + A' x + B' on E'
 __device__ __forceinline__ fp g_iso(const fp& x) {
@@ -174,7 +144,7 @@ __device__ __forceinline__ fp g_iso(const fp& x) {
 __device__ __forceinline__ bool sqrt_ratio(const fp& u, const fp& v, fp& y) {
     const fp tv2 = fp_mul(u, v);
     const fp tv1 = fp_mul(fp_sqr(v), tv2);                          // u v^3
-    const fp y1 = fp_mul(hpow(tv1, kSqrtRatioE, kSqrtRatioBits), tv2);
+    const fp y1 = fp_mul(fp_pow_ool(tv1, kSqrtRatioE, kSqrtRatioBits), tv2);
     const bool qr = fp_eq(fp_mul(fp_sqr(y1), v), u);
     y = qr ? y1 : fp_mul(y1, fp_load_u64(kSqrtMinusZ));
     return qr;
@@ -208,8 +178,8 @@ __device__ __forceinline__ fp horner_h(const uint64_t* c, int len, bool monic, c
     const int deg = len - 1 + (monic ? 1 : 0);
     fp acc = monic ? fp_one() : fp_load_u64(c + 6 * (len - 1)), dk = D;
     for (int i = deg - 1; i >= 0; --i) {
-        acc = fp_add(hmul(acc, N), hmul(fp_load_u64(c + 6 * i), dk));
-        dk = hmul(dk, D);
+        acc = fp_add(fp_mul_ool(acc, N), fp_mul_ool(fp_load_u64(c + 6 * i), dk));
+        dk = fp_mul_ool(dk, D);
     }
     return acc;
 }
@@ -245,7 +215,7 @@ static __device__ __noinline__ void neg_clear(const g1j& p0, const g1j& p1, fp& 
     const g1j q = g1j_add(p0, p1);
     g1j r = q;
     for (int i = 62; i >= 0; --i) {
-        r = hdbl(r);
+        r = g1j_dbl(r);
         if ((kHEff >> i) & 1) r = g1j_add(r, q);
     }
     fp rx, ry;
