@@ -343,6 +343,7 @@ __device__ __forceinline__ fp fp_pow_u64(const fp& a, const uint64_t* e, int nbi
 // nothing hides a miss in the instruction cache, and a loop that inlines a
 // multiply of several hundred instructions at every use misses on each pass.
 static __device__ __noinline__ fp fp_mul_ool(const fp& a, const fp& b) { return fp_mul(a, b); }
+__device__ __forceinline__ fp fp_sqr_ool(const fp& a) { return fp_mul_ool(a, a); }
 __device__ __forceinline__ fp fp_pow_ool(const fp& a, const uint64_t* e, int nbits) {
     fp r = fp_one(), base = a;
     for (int i = 0; i < nbits; ++i) {

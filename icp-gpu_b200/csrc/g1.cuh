@@ -55,8 +55,6 @@ struct g1j { fp X, Y, Z; };
 
 // The Jacobian routines run one thread per point, a few warps per scheduler:
 // their products are the out-of-line multiply of fp.cuh.
-__device__ __forceinline__ fp fp_sqr_ool(const fp& a) { return fp_mul_ool(a, a); }
-
 // dbl-2009-l (a = 0)
 static __device__ __noinline__ g1j g1j_dbl(const g1j& p) {
     fp A = fp_sqr_ool(p.X), B = fp_sqr_ool(p.Y), C = fp_sqr_ool(B);

@@ -4,8 +4,12 @@
 //   Fp12 = Fp6[w] / (w^2 - v)
 // Formulas follow the reference tower (gpu-crypto/cuda/field_sppark.cuh:52-197),
 // which mirrors ic_bls12_381 0.10.1: Karatsuba Fp2/Fp6/Fp12 products, the sparse
-// line product mul_by_014, Frobenius with fixed Montgomery constants, Fermat
-// inversion, and Granger-Scott squaring in the cyclotomic subgroup.  Every
+// line product mul_by_014, Frobenius with fixed Montgomery constants, the
+// inversion (binary extended Euclid, fp_inv.cuh; the reference's Fermat power
+// gives the same value), and Granger-Scott squaring in the cyclotomic
+// subgroup.  The tower keeps its products inline: the out-of-line multiply of
+// fp.cuh made the thread-per-verification kernel 20% faster but the key
+// ingest kernels (255 registers, large live state) up to 50% slower.  Every
 // value is canonical, so the final limbs equal the CPU verifier's bit for bit
 // whatever order the device evaluates the same formula in.
 #pragma once
