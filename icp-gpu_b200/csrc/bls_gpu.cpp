@@ -21,6 +21,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include <sys/random.h>
@@ -410,6 +411,72 @@ CtxView ctx_view(bls_ctx* c) {
                    c->d_g2, c->d_pk, c->d_pk_inf, c->n_pks, a.g2_norm, a.pk_norm, a.g2_corr, a.pk_corr};
 }
 }  // namespace bls
+
+namespace {
+
+// f(i) for i in [0, n) on up to 8 host threads
+template <class F>
+void host_parallel_for(int n, F f) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = std::max(1, std::min(n, (int)std::min(8u, hw ? hw : 1u)));
+    auto slice = [&](int t) {
+        for (int i = (int)((int64_t)n * t / nt); i < (int)((int64_t)n * (t + 1) / nt); ++i) f(i);
+    };
+    std::vector<std::thread> team;
+    for (int t = 1; t < nt; ++t) {
+        try {
+            team.emplace_back(slice, t);
+        } catch (...) {
+            slice(t);   // no thread to be had: this thread takes that slice too
+        }
+    }
+    slice(0);
+    for (auto& th : team) th.join();
+}
+
+// The reference's entry point takes one line table per item (19,584 B) and a
+// batch usually repeats a few keys many times.  The distinct tables are found
+// on the host: candidates by a fingerprint of each table's first words, every
+// match confirmed by comparing the whole table, so two different tables never
+// share an id.  idx[i]: the distinct table of item i; uniq[j]: an item whose
+// table is distinct table j.
+void distinct_tables(const uint64_t* tabs, int M, std::vector<int32_t>& idx, std::vector<int>& uniq) {
+    const size_t W = bls::kCoeffU64;
+    std::vector<uint64_t> fp((size_t)M);
+    host_parallel_for(M, [&](int i) {
+        const uint64_t* t = tabs + W * (size_t)i;
+        uint64_t h = 0xcbf29ce484222325ULL;
+        for (int k = 0; k < 12; ++k) h = (h ^ t[k]) * 0x100000001b3ULL;
+        fp[i] = h;
+    });
+    idx.assign((size_t)M, -1);
+    uniq.clear();
+    std::vector<int32_t> cand((size_t)M, -1);
+    std::unordered_map<uint64_t, int32_t> first;
+    first.reserve((size_t)M);
+    for (int i = 0; i < M; ++i) {
+        auto it = first.emplace(fp[i], (int32_t)uniq.size());
+        if (it.second) {
+            idx[i] = (int32_t)uniq.size();
+            uniq.push_back(i);
+        } else {
+            cand[i] = it.first->second;
+        }
+    }
+    std::vector<char> differs((size_t)M, 0);
+    host_parallel_for(M, [&](int i) {
+        if (cand[i] < 0) return;
+        if (memcmp(tabs + W * (size_t)i, tabs + W * (size_t)uniq[cand[i]], W * 8) == 0) idx[i] = cand[i];
+        else differs[i] = 1;
+    });
+    for (int i = 0; i < M; ++i) {   // a fingerprint shared by different tables: a table of its own
+        if (!differs[i]) continue;
+        idx[i] = (int32_t)uniq.size();
+        uniq.push_back(i);
+    }
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -999,28 +1066,46 @@ int gpu_batch_bls_verify(const uint64_t* sigs, const uint64_t* neg_hms, const ui
     auto body = [&]() -> int {
         CK(cudaSetDevice(c->cfg.device));
         size_t n = (size_t)M;
+        const size_t W = bls::kCoeffU64;
+        // repeated keys: only the distinct tables cross, with an item -> table
+        // index; mostly distinct tables cross whole (no index)
+        std::vector<int32_t> idx;
+        std::vector<int> uniq;
+        distinct_tables(pk_coeffs, M, idx, uniq);
+        const bool indexed = 2 * uniq.size() <= n;
+        const size_t ntab = indexed ? uniq.size() : n;
         int rc;
         if ((rc = c->grow(c->d_sigs, n * 96)) || (rc = c->grow(c->d_nhms, n * 96)) ||
-            (rc = c->grow(c->d_pk_items, n * bls::kCoeffU64 * 8)) || (rc = c->grow(c->d_g2_call, bls::kCoeffU64 * 8)) ||
-            (rc = c->grow(c->d_res, n * 4)))
+            (rc = c->grow(c->d_pk_items, ntab * W * 8)) || (rc = c->grow(c->d_g2_call, W * 8)) ||
+            (rc = c->grow(c->d_res, n * 4)) || (indexed && (rc = c->grow(c->d_pkidx, n * 4))))
             return rc;
         CK(cudaMemcpyAsync(c->d_sigs.p, sigs, n * 96, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->d_nhms.p, neg_hms, n * 96, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->d_g2_call.p, g2_coeffs, bls::kCoeffU64 * 8, cudaMemcpyHostToDevice, c->stream));
-        if ((rc = c->stage_h2d(c->d_pk_items.p, pk_coeffs, n * bls::kCoeffU64 * 8))) return rc;
+        CK(cudaMemcpyAsync(c->d_g2_call.p, g2_coeffs, W * 8, cudaMemcpyHostToDevice, c->stream));
+        std::vector<uint64_t> gathered;
+        if (indexed) {
+            gathered.resize(ntab * W);
+            host_parallel_for((int)ntab, [&](int j) {
+                memcpy(gathered.data() + W * (size_t)j, pk_coeffs + W * (size_t)uniq[j], W * 8);
+            });
+            if ((rc = c->stage_h2d(c->d_pk_items.p, gathered.data(), ntab * W * 8))) return rc;
+            CK(cudaMemcpyAsync(c->d_pkidx.p, idx.data(), n * 4, cudaMemcpyHostToDevice, c->stream));
+        } else if ((rc = c->stage_h2d(c->d_pk_items.p, pk_coeffs, n * W * 8))) {
+            return rc;
+        }
         bls::VerifyArgs a{};
         a.sigs = c->d_sigs.p;
         a.sig_compressed = 0;
         a.nhms = (const uint64_t*)c->d_nhms.p;
         a.g2 = (const uint64_t*)c->d_g2_call.p;
         a.pk_tables = (const uint64_t*)c->d_pk_items.p;
-        a.pk_index = nullptr;
+        a.pk_index = indexed ? (const int32_t*)c->d_pkidx.p : nullptr;
         a.pk_identity = nullptr;
         a.n = M;
         a.results = (int32_t*)c->d_res.p;
         if ((rc = run_verify(c, a))) return rc;
         CK(cudaMemcpyAsync(results, a.results, n * 4, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
+        CK(cudaStreamSynchronize(c->stream));   // also keeps `gathered` and `idx` alive until their copies end
         return BLS_OK;
     };
     return body() == BLS_OK ? 0 : -1;

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import bls_gpu as G
+import cpu as C
 import workload_py as W
 
 pytestmark = pytest.mark.gpu
@@ -92,3 +93,28 @@ def test_shared_context_concurrent_callers(ctx, big):
             r = ctx.verify(big["sigs"][a:b], big["nhms"][a:b], ids[a:b])
             assert (r == big["expect"][a:b]).all()
     _run_threads(call, 4)
+
+
+def test_reference_abi_repeated_tables(golden, big):
+    """4,096 items over 40 keys through the reference's entry point: one table
+    per item, repeated; the library copies the distinct ones with an index."""
+    n = 4096
+    tabs = np.ascontiguousarray(big["pk_tables"][big["pk_index"][:n]])
+    got = G.batch_bls_verify(big["sigs"][:n], big["nhms"][:n], golden["g2_gen_coeffs"], tabs)
+    assert [int(x) for x in got] == list(big["expect"][:n])
+
+
+def test_reference_abi_fingerprint_twins(golden, big):
+    """Tables equal to a key's table except in the last word share its
+    fingerprint but must not share its id: every result equals the oracle's on
+    the same per-item tables."""
+    n = 600
+    tabs = np.ascontiguousarray(big["pk_tables"][big["pk_index"][:n]])
+    twins = np.arange(3, n, 7)
+    tabs[twins, -1] ^= np.uint64(1)
+    got = np.array(G.batch_bls_verify(big["sigs"][:n], big["nhms"][:n], golden["g2_gen_coeffs"], tabs),
+                   dtype=np.int32)
+    want = C.verify_batch(big["sigs"][:n], big["nhms"][:n], golden["g2_gen_coeffs"], tabs, nthreads=8)
+    assert (got == want).all()
+    untouched = np.setdiff1d(np.arange(n), twins)
+    assert (got[untouched] == big["expect"][untouched]).all()
