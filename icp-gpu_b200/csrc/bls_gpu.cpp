@@ -156,6 +156,13 @@ struct bls_ctx {
         return BLS_OK;
     }
 
+    // The reference entry point's key tables seen before, kept on the device
+    // as registered keys (ids in d_pk / d_pk_norm) and found again by exact
+    // content: fingerprint -> ids, with a host copy of every cached table.
+    std::unordered_multimap<uint64_t, int32_t> table_ids;
+    std::vector<uint64_t> h_cached;   // table of key id k at k * 2448 (ids below n_pks)
+    std::vector<uint64_t> h_g2_table; // the generator table d_g2 holds, fetched on first use
+
     // Large host inputs (the reference entry point's per-item line tables,
     // 19,584 B an item) copy from pageable memory at a fraction of the link's
     // rate, so they go through two pinned staging buffers in turn: a team of
@@ -440,15 +447,16 @@ void host_parallel_for(int n, F f) {
 // match confirmed by comparing the whole table, so two different tables never
 // share an id.  idx[i]: the distinct table of item i; uniq[j]: an item whose
 // table is distinct table j.
+uint64_t table_fingerprint(const uint64_t* t) {   // the first 12 words (FNV-1a over words)
+    uint64_t h = 0xcbf29ce484222325ULL;
+    for (int k = 0; k < 12; ++k) h = (h ^ t[k]) * 0x100000001b3ULL;
+    return h;
+}
+
 void distinct_tables(const uint64_t* tabs, int M, std::vector<int32_t>& idx, std::vector<int>& uniq) {
     const size_t W = bls::kCoeffU64;
     std::vector<uint64_t> fp((size_t)M);
-    host_parallel_for(M, [&](int i) {
-        const uint64_t* t = tabs + W * (size_t)i;
-        uint64_t h = 0xcbf29ce484222325ULL;
-        for (int k = 0; k < 12; ++k) h = (h ^ t[k]) * 0x100000001b3ULL;
-        fp[i] = h;
-    });
+    host_parallel_for(M, [&](int i) { fp[i] = table_fingerprint(tabs + W * (size_t)i); });
     idx.assign((size_t)M, -1);
     uniq.clear();
     std::vector<int32_t> cand((size_t)M, -1);
@@ -474,6 +482,54 @@ void distinct_tables(const uint64_t* tabs, int M, std::vector<int32_t>& idx, std
         idx[i] = (int32_t)uniq.size();
         uniq.push_back(i);
     }
+}
+
+// Key ids for the distinct tables of a reference-entry call (tables[j] =
+// the caller's table of distinct table j): cached ones found by exact content,
+// new ones registered in one contiguous block and normalised in one launch.
+// False (nothing changed) when the key store has no room for the new ones.
+bool cached_table_ids(bls_ctx* c, const std::vector<const uint64_t*>& tables, std::vector<int32_t>& ids, int* rc) {
+    const size_t W = bls::kCoeffU64;
+    *rc = BLS_OK;
+    ids.assign(tables.size(), -1);
+    std::vector<int> fresh;   // distinct tables not cached yet
+    for (size_t j = 0; j < tables.size(); ++j) {
+        const auto range = c->table_ids.equal_range(table_fingerprint(tables[j]));
+        for (auto it = range.first; it != range.second && ids[j] < 0; ++it)
+            if (memcmp(tables[j], c->h_cached.data() + W * (size_t)it->second, W * 8) == 0) ids[j] = it->second;
+        if (ids[j] < 0) fresh.push_back((int)j);
+    }
+    if (fresh.empty()) return true;
+    if (c->n_pks + (int)fresh.size() > c->cfg.max_pks) return false;
+    const int first = c->n_pks;
+    const size_t k = fresh.size();
+    c->h_cached.resize(W * (size_t)(first + (int)k));
+    for (size_t f = 0; f < k; ++f)
+        memcpy(c->h_cached.data() + W * (size_t)(first + (int)f), tables[fresh[f]], W * 8);
+    auto ck = [&](cudaError_t e) {
+        if (e != cudaSuccess && *rc == BLS_OK) *rc = fail(BLS_ERR_CUDA, "%s", cudaGetErrorString(e));
+        return e == cudaSuccess;
+    };
+    std::vector<uint8_t> bad(k, 0);
+    if (!ck(cudaMemcpyAsync(c->d_pk + W * (size_t)first, c->h_cached.data() + W * (size_t)first, k * W * 8,
+                            cudaMemcpyHostToDevice, c->stream)) ||
+        !ck(cudaMemsetAsync(c->d_pk_inf + first, 0, k, c->stream)) ||
+        !ck(bls::launch_lines_normalize(c->d_pk + W * (size_t)first, (int)k, c->d_pk_norm + W * (size_t)first,
+                                        c->d_corr + 12 * (size_t)(1 + first), c->d_norm_bad + 1 + first,
+                                        c->stream)) ||
+        !ck(cudaMemcpyAsync(bad.data(), c->d_norm_bad + 1 + first, k, cudaMemcpyDeviceToHost, c->stream)) ||
+        !ck(cudaStreamSynchronize(c->stream))) {
+        c->h_cached.resize(W * (size_t)first);
+        return false;
+    }
+    for (size_t f = 0; f < k; ++f) {
+        if (bad[f]) c->norm_ok = false;   // a table with a zero c2: the raw-table path from now on
+        c->h_pk_inf[first + (int)f] = 0;
+        c->table_ids.emplace(table_fingerprint(tables[fresh[f]]), first + (int)f);
+        ids[fresh[f]] = first + (int)f;
+    }
+    c->n_pks += (int)k;
+    return true;
 }
 
 }  // namespace
@@ -1082,6 +1138,39 @@ int gpu_batch_bls_verify(const uint64_t* sigs, const uint64_t* neg_hms, const ui
         CK(cudaMemcpyAsync(c->d_sigs.p, sigs, n * 96, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->d_nhms.p, neg_hms, n * 96, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->d_g2_call.p, g2_coeffs, W * 8, cudaMemcpyHostToDevice, c->stream));
+        // a repeat call over tables seen before: registered keys, normalised
+        // lines, nothing but the index crosses (the caller's generator table
+        // must be the one the context holds)
+        if (indexed) {
+            if (c->h_g2_table.empty()) {
+                c->h_g2_table.resize(W);
+                CK(cudaMemcpyAsync(c->h_g2_table.data(), c->d_g2, W * 8, cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
+            std::vector<const uint64_t*> tables(uniq.size());
+            for (size_t j = 0; j < uniq.size(); ++j) tables[j] = pk_coeffs + W * (size_t)uniq[j];
+            std::vector<int32_t> ids;
+            if (memcmp(g2_coeffs, c->h_g2_table.data(), W * 8) == 0 && cached_table_ids(c, tables, ids, &rc)) {
+                for (size_t i = 0; i < n; ++i) idx[i] = ids[idx[i]];
+                CK(cudaMemcpyAsync(c->d_pkidx.p, idx.data(), n * 4, cudaMemcpyHostToDevice, c->stream));
+                bls::VerifyArgs a{};
+                a.sigs = c->d_sigs.p;
+                a.sig_compressed = 0;
+                a.nhms = (const uint64_t*)c->d_nhms.p;
+                a.g2 = c->d_g2;
+                a.pk_tables = c->d_pk;
+                c->set_norm(a);
+                a.pk_index = (const int32_t*)c->d_pkidx.p;
+                a.pk_identity = c->d_pk_inf;
+                a.n = M;
+                a.results = (int32_t*)c->d_res.p;
+                if ((rc = run_verify(c, a))) return rc;
+                CK(cudaMemcpyAsync(results, a.results, n * 4, cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+                return BLS_OK;
+            }
+            if (rc) return rc;
+        }
         std::vector<uint64_t> gathered;
         if (indexed) {
             gathered.resize(ntab * W);

@@ -118,3 +118,31 @@ def test_reference_abi_fingerprint_twins(golden, big):
     assert (got == want).all()
     untouched = np.setdiff1d(np.arange(n), twins)
     assert (got[untouched] == big["expect"][untouched]).all()
+
+
+def test_reference_abi_repeat_call_uses_cached_tables(golden, big):
+    """The same tables again (found by exact content among the tables seen
+    before, so nothing but the index crosses), then a batch mixing cached and
+    new tables: the same results as the first call and the oracle."""
+    n = 3000
+    tabs = np.ascontiguousarray(big["pk_tables"][big["pk_index"][:n]])
+    for _ in range(2):
+        got = G.batch_bls_verify(big["sigs"][:n], big["nhms"][:n], golden["g2_gen_coeffs"], tabs)
+        assert [int(x) for x in got] == list(big["expect"][:n])
+    mixed = tabs.copy()
+    mixed[::5, 100] ^= np.uint64(1 << 7)     # some tables the library has not seen
+    got = np.array(G.batch_bls_verify(big["sigs"][:n], big["nhms"][:n], golden["g2_gen_coeffs"], mixed),
+                   dtype=np.int32)
+    want = C.verify_batch(big["sigs"][:n], big["nhms"][:n], golden["g2_gen_coeffs"], mixed, nthreads=8)
+    assert (got == want).all()
+
+
+def test_reference_abi_other_generator_table(golden, big):
+    """A caller's generator table that is not the context's own: the tables
+    cross as they are and the results equal the oracle's with that table."""
+    n = 400
+    tabs = np.ascontiguousarray(big["pk_tables"][big["pk_index"][:n]])
+    g2 = golden["pk42_coeffs"]
+    got = np.array(G.batch_bls_verify(big["sigs"][:n], big["nhms"][:n], g2, tabs), dtype=np.int32)
+    want = C.verify_batch(big["sigs"][:n], big["nhms"][:n], g2, tabs, nthreads=8)
+    assert (got == want).all()
