@@ -342,7 +342,7 @@ def run_gpu(args):
         hashing = run_hash(G, WL, ctx, wl, pk_ids)
         compressed = run_compressed(G, WL, ctx, n=args.compressed_items) if args.compressed_items > 0 else None
         rlc = run_rlc(G, WL, ctx, wl, pk_ids, n=args.rlc_items) if args.rlc_items > 0 else None
-        batching = run_batching(G, WL, ctx, ids)
+        batching = run_batching(G, WL, ctx, wl)
         if args.serve_seconds > 0:
             serving = run_serving(G, WL, ctx, args.serve_seconds, slots=args.serve_slots,
                                   max_batch=args.serve_max_batch, mode=args.serve_mode,
@@ -470,10 +470,13 @@ def run_compressed(G, WL, ctx, n=65536, reps=3):
     return out
 
 
-def run_batching(G, WL, ctx, ids_unused, reps=2):
+def run_batching(G, WL, ctx, wl_headline, reps=2):
     """Batching workload: 256 requests, sizes log-uniform in [1, 2048], 1-40 keys each;
     one launch per request against one persistent graph-replayed launch, both
-    through bls_verify_requests from host buffers (host-timed, best of reps)."""
+    through bls_verify_requests from host buffers (host-timed, best of reps).
+    Then the autotuner's sweep (bls_autotune: lanes per verification x blocks
+    per SM, each timed on the headline workload resident on the device) on a
+    context of its own, since the sweep keeps its choice in the context."""
     wl = WL.config_requests(256, 2048, N_KEYS, seed=4)
     ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
     off = wl["offsets"]
@@ -491,6 +494,26 @@ def run_batching(G, WL, ctx, ids_unused, reps=2):
         out[name + "_verifies_per_s"] = round(n / best, 1)
         out[name + "_ms"] = round(best * 1e3, 2)
     out["speedup"] = round(out["persistent_verifies_per_s"] / out["plain_verifies_per_s"], 2)
+
+    import torch
+    tctx = G.Context()
+    try:
+        tids = np.array([tctx.register_pk_affine(q) for q in wl_headline["pk_affine"]],
+                        dtype=np.int32)[wl_headline["pk_index"]]
+        dev = torch.device("cuda", torch.cuda.current_device())
+        ds = torch.from_numpy(wl_headline["sigs"].view(np.int64)).to(dev)
+        dn = torch.from_numpy(wl_headline["nhms"].view(np.int64)).to(dev)
+        di = torch.from_numpy(tids).to(dev)
+        pts = tctx.autotune(len(tids), ds.data_ptr(), dn.data_ptr(), di.data_ptr(), repeats=2)
+    finally:
+        tctx.close()
+    lanes_name = {1: "thread per verification", 6: "Fp2 lanes (12 threads)"}
+    best = min(pts, key=lambda p: p[2])
+    out["autotune"] = {
+        "sample": "keyset-4096-40, inputs resident (bls_autotune, best of 2 per point)",
+        "points": [{"lanes": l, "kernel": lanes_name.get(l, "%d lanes" % l), "blocks_per_sm": b, "ms": round(ms, 3)}
+                   for l, b, ms in pts],
+        "chosen": {"lanes": best[0], "blocks_per_sm": best[1], "ms": round(best[2], 3)}}
     return out
 
 
