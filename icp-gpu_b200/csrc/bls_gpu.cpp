@@ -441,18 +441,19 @@ void host_parallel_for(int n, F f) {
     for (auto& th : team) th.join();
 }
 
-// The reference's entry point takes one line table per item (19,584 B) and a
-// batch usually repeats a few keys many times.  The distinct tables are found
-// on the host: candidates by a fingerprint of each table's first words, every
-// match confirmed by comparing the whole table, so two different tables never
-// share an id.  idx[i]: the distinct table of item i; uniq[j]: an item whose
-// table is distinct table j.
-uint64_t table_fingerprint(const uint64_t* t) {   // the first 12 words (FNV-1a over words)
+// a line table's fingerprint: FNV-1a over its first 12 words (candidates
+// only; equality is always decided by comparing whole tables)
+uint64_t table_fingerprint(const uint64_t* t) {
     uint64_t h = 0xcbf29ce484222325ULL;
     for (int k = 0; k < 12; ++k) h = (h ^ t[k]) * 0x100000001b3ULL;
     return h;
 }
 
+// The reference's entry point takes one line table per item (19,584 B) and a
+// batch usually repeats a few keys many times.  The distinct tables are found
+// on the host: candidates by fingerprint, every match confirmed by comparing
+// the whole table, so two different tables never share an id.  idx[i]: the
+// distinct table of item i; uniq[j]: an item whose table is distinct table j.
 void distinct_tables(const uint64_t* tabs, int M, std::vector<int32_t>& idx, std::vector<int>& uniq) {
     const size_t W = bls::kCoeffU64;
     std::vector<uint64_t> fp((size_t)M);
