@@ -103,6 +103,7 @@ def lib():
         L.bls_pk_register_coeffs.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_int32)]
         L.bls_pk_register_affine.argtypes = [P, P, ctypes.POINTER(ctypes.c_int32)]
         L.bls_pk_register_compressed.argtypes = [P, P, I, P, P]
+        L.bls_pk_register_affine_batch.argtypes = [P, P, I, P]
         L.bls_g2_decompress_status.argtypes = [P, P, I, P, P]
         L.bls_pk_table.argtypes = [P, ctypes.c_int32, P]
         L.bls_verify_batch.argtypes = [P, ctypes.POINTER(Batch), P]
@@ -116,7 +117,7 @@ def lib():
         L.bls_verify_batch_rlc.argtypes = [P, ctypes.POINTER(Batch), P, P, ctypes.POINTER(I), P]
         L.bls_verify_messages.argtypes = [P, I, P, P, P, P, I, P, I, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
-        L.bls_verify_compressed_noalloc.argtypes = [P, P, P, P, P, P, I, I, P]
+        L.bls_verify_compressed_noalloc.argtypes = [P, P, P, P, P, I, P, P, I, I, P]
         L.bls_server_create.argtypes = [P, ctypes.POINTER(ServerConfig), ctypes.POINTER(P)]
         L.bls_server_destroy.argtypes = [P]
         L.bls_server_destroy.restype = None
@@ -208,13 +209,14 @@ def g1_decompress_batch(compressed_points):
 NOALLOC_MAX_ITEMS = 8192
 
 
-def verify_compressed_noalloc(sigs48_ptr, nhms_ptr, g2_ptr, pk_tables_ptr, pk_index_ptr, results_ptr, n,
-                              lanes=8, stream=None):
+def verify_compressed_noalloc(sigs48_ptr, nhms_ptr, g2_ptr, pk_tables_ptr, pk_identity_ptr, n_tables, pk_index_ptr,
+                              results_ptr, n, lanes=6, stream=None):
     """Enqueue a verify of n compressed signatures on `stream` using only
-    caller-owned device buffers (raw device pointers); the library allocates
-    nothing.  Returns the library status code (0 = enqueued)."""
-    return lib().bls_verify_compressed_noalloc(sigs48_ptr, nhms_ptr, g2_ptr, pk_tables_ptr, pk_index_ptr,
-                                               results_ptr, n, lanes, stream)
+    caller-owned device buffers (raw device pointers; pk_identity_ptr may be
+    None); the library allocates nothing.  Returns the library status code
+    (0 = enqueued)."""
+    return lib().bls_verify_compressed_noalloc(sigs48_ptr, nhms_ptr, g2_ptr, pk_tables_ptr, pk_identity_ptr,
+                                               n_tables, pk_index_ptr, results_ptr, n, lanes, stream)
 
 
 class Context:
@@ -267,6 +269,14 @@ class Context:
         pid = ctypes.c_int32()
         self._check(self.lib.bls_pk_register_affine(self.h, _ptr(q), ctypes.byref(pid)), "bls_pk_register_affine")
         return pid.value
+
+    def register_pk_affine_batch(self, q24s):
+        """Register n affine keys ((n, 24) u64) in one call; returns their ids."""
+        q = _u64(q24s).reshape(-1, 24)
+        ids = np.full(q.shape[0], -1, dtype=np.int32)
+        self._check(self.lib.bls_pk_register_affine_batch(self.h, _ptr(q), q.shape[0], _ptr(ids)),
+                    "bls_pk_register_affine_batch")
+        return ids
 
     def register_pk_compressed(self, pks96):
         """Decode, validate and prepare n 96-byte keys on the GPU.  Returns

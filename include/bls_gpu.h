@@ -146,6 +146,11 @@ int bls_pk_register_coeffs(bls_ctx* ctx, const uint64_t* coeffs2448, int is_iden
 /* From an affine point (x.c0, x.c1, y.c0, y.c1: 24 x uint64 Montgomery); the
  * line table is computed on the GPU.  The caller vouches that the point is in G2. */
 int bls_pk_register_affine(bls_ctx* ctx, const uint64_t* q24, int32_t* pk_id);
+/* From n affine points at once (n x 24 uint64, each as for
+ * bls_pk_register_affine); pk_ids[i] gets key i's id.  One launch builds all n
+ * line tables and one normalises them, so registering a key set costs about
+ * what one key costs.  The caller vouches that every point is in G2. */
+int bls_pk_register_affine_batch(bls_ctx* ctx, const uint64_t* q24, int n, int32_t* pk_ids);
 /* From n 96-byte compressed keys (ZCash encoding: x.c1 || x.c0 big-endian,
  * flags in byte 0 as for G1; x^3 + 4(1 + u) must be a square in Fp2 and the
  * point in G2).  Decoding, every G2Affine::from_compressed check, the line
@@ -261,23 +266,32 @@ int bls_server_stats(bls_server* srv, uint64_t* launches, uint64_t* items, uint6
 /* ---- verification without device allocation ----
  * No counterpart in the reference: its wrapper allocates and frees device
  * memory on every call (gpu-crypto/cuda/api.cu:137-159).  For callers that
- * cannot call cudaMalloc while they verify -- code inside a CUDA stream
- * capture, plugins whose host hands all device memory to its own allocator,
- * latency-critical paths that cannot afford cudaMalloc's device-wide
- * synchronisation.  Every pointer is device memory owned by the caller:
- * sigs48 (n x 48 B), neg_hms (n x 12 u64), g2_coeffs (2448 u64), pk_tables
- * (k x 2448 u64), pk_index (n), results (n, as bls_verify_batch).  The work is
- * enqueued on `stream` (a cudaStream_t) and not synchronised.  Scratch lives
- * in a fixed device array inside the library (about 0.8 MB on each GPU that
- * loads it, held until exit), so at most BLS_NOALLOC_MAX_ITEMS items per call
- * (more returns BLS_ERR_INVALID).  All calls on a device share that array:
- * calls whose work overlaps on the GPU race and must be ordered by the
- * caller.  The first call on a device looks up the array's address; make it
- * before any stream capture.  lanes_per_pairing: 2, 4, 6 or 8. */
+ * cannot call cudaMalloc while they verify: plugins whose host process hands
+ * all device memory to its own allocator (a framework's caching allocator, a
+ * fixed per-tenant budget), and latency-critical paths that cannot afford
+ * cudaMalloc's device-wide synchronisation.  Every pointer is device memory
+ * owned by the caller: sigs48 (n x 48 B), neg_hms (n x 12 u64), g2_coeffs
+ * (2448 u64), pk_tables (n_tables x 2448 u64), pk_identity (optional,
+ * n_tables bytes, nonzero marks an identity key, which contributes nothing to
+ * the Miller loop as in bls_pk_register_coeffs; NULL = no identity key),
+ * pk_index (n), results (n, as bls_verify_batch, and
+ * -BLS_ST_BAD_KEY_INDEX for an item whose pk_index is outside
+ * [0, n_tables); no table is read for it).  The work is enqueued on `stream`
+ * (a cudaStream_t) and not synchronised.  Scratch lives in a fixed device
+ * array inside the library (about 0.85 MB on each GPU that loads it, held
+ * until exit), so at most BLS_NOALLOC_MAX_ITEMS items per call (more returns
+ * BLS_ERR_INVALID).  All calls on a device share that array: calls whose work
+ * overlaps on the GPU race and must be ordered by the caller.  The first call
+ * on a device does the set-up (looks up the array's address, sets the verify
+ * kernel's shared-memory attribute); make it before any stream capture, and
+ * do not use this entry point across a cudaDeviceReset (the cached address
+ * goes stale).  lanes_per_pairing: 2, 4, 6 or 8. */
 #define BLS_NOALLOC_MAX_ITEMS 8192
+#define BLS_ST_BAD_KEY_INDEX 5     /* bls_verify_compressed_noalloc: key index outside the caller's tables */
 int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64_t* neg_hms, const uint64_t* g2_coeffs,
-                                  const uint64_t* pk_tables, const int32_t* pk_index, int32_t* results, int n,
-                                  int lanes_per_pairing, void* stream);
+                                  const uint64_t* pk_tables, const uint8_t* pk_identity, int n_tables,
+                                  const int32_t* pk_index, int32_t* results, int n, int lanes_per_pairing,
+                                  void* stream);
 
 /* Random-linear-combination batch verification (opt-in): one combined check
  *   e(sum r_i sig_i, G2) * prod_k e(sum_{pk_i = k} r_i (-H(m_i)), pk_k) == 1
