@@ -204,7 +204,6 @@ struct bls_server {
             cudaEventRecord(ring.done, ring.kern))
             return BLS_ERR_CUDA;
         ring.launched = true;
-        ++launches;
         return BLS_OK;
     }
 
@@ -220,9 +219,14 @@ struct bls_server {
         return BLS_OK;
     }
 
-    // one pass: results of the in-flight range, completions, admissions and
-    // their publication, (re)launch; `progressed` when anything moved
-    int ring_step(bool& progressed) {
+    // One pass: results of the in-flight range, completions, admissions and
+    // their publication, (re)launch; `progressed` when anything moved.  Only
+    // the dispatcher thread touches the ring and its flights; the server mutex
+    // (`lk`, held on entry and on return) guards the queue, the completion map
+    // and the counters, and is released around every device round trip so
+    // that submitters and waiters never queue behind a copy or a sync.
+    int ring_step(std::unique_lock<std::mutex>& lk, bool& progressed) {
+        lk.unlock();
         const uint32_t inflight = ring.pub - ring.tail;
         if (inflight) {
             const uint32_t s0 = ring.tail % ring.cap, first = std::min(inflight, ring.cap - s0);
@@ -230,11 +234,14 @@ struct bls_server {
                                 ring.copy) ||
                 (first < inflight && cudaMemcpyAsync(ring.h_res, ring.d_res, 4 * (size_t)(inflight - first),
                                                      cudaMemcpyDeviceToHost, ring.copy)) ||
-                cudaStreamSynchronize(ring.copy))
+                cudaStreamSynchronize(ring.copy)) {
+                lk.lock();
                 return BLS_ERR_CUDA;
+            }
         }
         const int64_t t = now_ns();
-        bool any_done = false;
+        std::vector<uint64_t> finished;
+        uint64_t finished_items = 0;
         for (auto& f : ring.flights) {
             if (f.complete) continue;
             bool all = true;
@@ -245,24 +252,36 @@ struct bls_server {
                 }
             if (!all) continue;
             for (int k = 0; k < f.req.n; ++k) f.req.results[k] = ring.h_res[(f.start + k) % ring.cap];
-            done[f.req.ticket] = t;
-            items += f.req.n;
+            finished.push_back(f.req.ticket);
+            finished_items += f.req.n;
             f.complete = true;
-            any_done = true;
         }
         while (!ring.flights.empty() && ring.flights.front().complete) {
             ring.tail += ring.flights.front().span;
             ring.flights.pop_front();
         }
-        if (any_done) {
+        // completions out, admissions in: the only part under the mutex
+        std::vector<Pending> admit;
+        uint32_t room = ring.cap - (ring.pub - ring.tail);
+        lk.lock();
+        for (uint64_t tk : finished) done[tk] = t;
+        items += finished_items;
+        while (!queue.empty()) {
+            const uint32_t span = ((uint32_t)queue.front().n + kGroup - 1) / kGroup * kGroup;
+            if (span > room) break;
+            room -= span;
+            if ((uint64_t)queue.front().n > max_batch) max_batch = queue.front().n;
+            admit.push_back(std::move(queue.front()));
+            queue.pop_front();
+        }
+        lk.unlock();
+        if (!finished.empty()) {
             cv_done.notify_all();
             progressed = true;
         }
         const uint32_t from = ring.pub;
-        while (!queue.empty()) {
-            Pending& q = queue.front();
+        for (Pending& q : admit) {
             const uint32_t span = ((uint32_t)q.n + kGroup - 1) / kGroup * kGroup;
-            if (ring.pub - ring.tail + span > ring.cap) break;
             for (uint32_t k = 0; k < span; ++k) {
                 const uint32_t slot = (ring.pub + k) % ring.cap;
                 ring.h_res[slot] = kSentinel;
@@ -276,41 +295,45 @@ struct bls_server {
                     ring.h_ids[slot] = 0;
                 }
             }
-            if ((uint64_t)q.n > max_batch) max_batch = q.n;
             ring.flights.push_back(Ring::Flight{std::move(q), ring.pub, span, false});
             ring.pub += span;
-            queue.pop_front();
         }
+        int rc = BLS_OK;
         if (ring.pub != from) {
             const uint32_t n = ring.pub - from;
-            int rc;
             if ((rc = ring_copy_in(ring.d_sigs, ring.h_sigs, 12, from, n)) ||
                 (rc = ring_copy_in(ring.d_nhms, ring.h_nhms, 12, from, n)) ||
                 (rc = ring_copy_in(ring.d_ids, ring.h_ids, 1, from, n)) ||
-                (rc = ring_copy_in(ring.d_res, ring.h_res, 1, from, n)))
+                (rc = ring_copy_in(ring.d_res, ring.h_res, 1, from, n))) {
+                lk.lock();
                 return rc;
+            }
             // the count goes up only after the items' copies (same stream)
             ring.h_ctl[0] = ring.pub;
             if (cudaMemcpyAsync(ring.d_ctl, ring.h_ctl, 4, cudaMemcpyHostToDevice, ring.copy) ||
-                cudaStreamSynchronize(ring.copy))
+                cudaStreamSynchronize(ring.copy)) {
+                lk.lock();
                 return BLS_ERR_CUDA;
+            }
             progressed = true;
         }
-        bool pending = false;
+        bool pending = false, relaunched = false;
         for (auto& f : ring.flights) pending = pending || !f.complete;
         if (pending && !(ring.launched && cudaEventQuery(ring.done) == cudaErrorNotReady)) {
-            int rc = ring_launch();
-            if (rc) return rc;
+            rc = ring_launch();
+            relaunched = rc == BLS_OK;
             progressed = true;
         }
-        return BLS_OK;
+        lk.lock();
+        if (relaunched) ++launches;
+        return rc;
     }
 
     void run_ring() {
         std::unique_lock<std::mutex> lk(mu);
         while (true) {
             bool progressed = false;
-            int rc = ring_step(progressed);
+            int rc = ring_step(lk, progressed);
             if (rc) {
                 error = rc;
                 cv_done.notify_all();

@@ -363,6 +363,16 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     return t;
 }
 
+// the published count with acquire semantics at GPU scope: the ring items
+// that the host's copies wrote before the count are visible to this thread's
+// later loads (and, through the block barrier that follows the claim, to the
+// block's other threads)
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const volatile uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // Ring serving, thread 0 of a block: claim the next published group of five
 // items (all in device memory).  False when the block should leave: the stop
 // flag, serve_idle_ns in which the published count did not move (idle for the
@@ -371,12 +381,15 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 // also has an iteration cap, so every wait ends.
 __device__ bool serve_claim(const VerifyArgs& a, uint64_t t_launch, uint32_t* base) {
     uint64_t t_moved = globaltimer_ns();
-    uint32_t seen = *a.serve_avail;
+    uint32_t seen = ld_acquire_gpu(a.serve_avail);
     for (uint32_t it = 0; it < (1u << 26); ++it) {
         const uint32_t cur = *reinterpret_cast<volatile uint32_t*>(a.serve_claimed);
-        const uint32_t av = *a.serve_avail;
+        const uint32_t av = ld_acquire_gpu(a.serve_avail);
         if ((int32_t)(av - cur) > 0) {
             if (atomicCAS(a.serve_claimed, cur, cur + kPairsPerBlock) == cur) {
+                // order the claimed group's input loads after the count that
+                // published it
+                __threadfence();
                 *base = cur;
                 return true;
             }
@@ -469,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
         if (have) {
             const uint64_t* s = a.sig_xy ? a.sig_xy + 12 * (size_t)item : (const uint64_t*)a.sigs + 12 * (size_t)item;
             const uint64_t* h = a.nhms + 12 * (size_t)item;
-            if (in_status) status = (int32_t)in_status[item];
+            if (in_status) status = (int32_t)__ldcg(in_status + item);
             fp sx = fp_load_u64_cg(s), sy = fp_load_u64_cg(s + 6);
             fp hx = fp_load_u64_cg(h), hy = fp_load_u64_cg(h + 6);
             int64_t pki = a.pk_index ? (int64_t)__ldcg(a.pk_index + item) : (int64_t)item;
