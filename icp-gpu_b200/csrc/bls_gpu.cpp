@@ -622,6 +622,39 @@ int bls_pk_register_affine(bls_ctx* ctx, const uint64_t* q24, int32_t* pk_id) {
     return BLS_OK;
 }
 
+// Keys n_pks .. n_pks + n - 1 from affine points: one copy, one launch of the
+// line-table kernel and one of the normalisation for all n keys (the single
+// key form above costs a launch pair per key).
+int bls_pk_register_affine_batch(bls_ctx* ctx, const uint64_t* q24, int n, int32_t* pk_ids) {
+    if (!ctx || (n > 0 && (!q24 || !pk_ids))) return fail(BLS_ERR_INVALID, "NULL argument");
+    if (n < 0) return fail(BLS_ERR_INVALID, "n < 0");
+    if (n == 0) return BLS_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n > ctx->cfg.max_pks - ctx->n_pks)
+        return fail(BLS_ERR_FULL, "%d keys do not fit: %d of %d pk slots used", n, ctx->n_pks, ctx->cfg.max_pks);
+    CK(cudaSetDevice(ctx->cfg.device));
+    const size_t k = (size_t)n;
+    int rc = ctx->grow(ctx->d_in, k * 24 * 8);
+    if (rc) return rc;
+    const int id0 = ctx->n_pks;
+    uint64_t* tables = ctx->d_pk + (size_t)id0 * bls::kCoeffU64;
+    std::vector<uint8_t> bad(k);
+    CK(cudaMemcpyAsync(ctx->d_in.p, q24, k * 24 * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(bls::launch_g2_prepare((const uint64_t*)ctx->d_in.p, n, tables, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_pk_inf + id0, 0, k, ctx->stream));
+    CK(bls::launch_lines_normalize(tables, n, ctx->d_pk_norm + (size_t)id0 * bls::kCoeffU64,
+                                   ctx->d_corr + 12 * (size_t)(1 + id0), ctx->d_norm_bad + 1 + id0, ctx->stream));
+    CK(cudaMemcpyAsync(bad.data(), ctx->d_norm_bad + 1 + id0, k, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < k; ++i) {
+        ctx->h_pk_inf[id0 + i] = 0;
+        if (bad[i]) ctx->norm_ok = false;
+        pk_ids[i] = id0 + (int32_t)i;
+    }
+    ctx->n_pks += n;
+    return BLS_OK;
+}
+
 // Keys n_pks .. n_pks + n - 1 are decoded, prepared and normalised on the
 // device in one launch each; nothing is registered unless every key decodes.
 int bls_pk_register_compressed(bls_ctx* ctx, const uint8_t* pks96, int n, int32_t* pk_ids, int32_t* status) {

@@ -234,3 +234,26 @@ def test_identity_key(ctx, golden):
                                     want_values=True)
     assert res.tolist() == want.tolist() == [1, 0, 0]
     assert (ml == wml).all() and (gt == wgt).all()
+
+
+@pytest.mark.gpu
+def test_register_affine_batch_tables_pinned(ctx, golden, keys):
+    """n affine keys in one call (one launch of the table kernel and one of the
+    normalisation): the same tables as the reference's golden ones and the
+    workload's, consecutive ids, and the same verify results as keys
+    registered one at a time."""
+    (x0, x1), (y0, y1) = B.g2_mul(B.G2_GEN, 42)
+    q42 = np.array(B.mont_limbs(x0) + B.mont_limbs(x1) + B.mont_limbs(y0) + B.mont_limbs(y1), dtype=np.uint64)
+    qs = np.concatenate([q42[None], keys["q"]])
+    ids = ctx.register_pk_affine_batch(qs)
+    assert list(ids) == list(range(ids[0], ids[0] + len(ids)))
+    assert (ctx.pk_table(int(ids[0])) == golden["pk42_coeffs"]).all()
+    for i in range(keys["q"].shape[0]):
+        assert (ctx.pk_table(int(ids[1 + i])) == keys["tables"][i]).all()
+    wl = W.plain_config(n=64, seed=4)
+    batch_ids = ctx.register_pk_affine_batch(wl["pk_affine"])
+    single_ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
+    a = ctx.verify(wl["sigs"], wl["nhms"], batch_ids)
+    b = ctx.verify(wl["sigs"], wl["nhms"], single_ids)
+    assert (a == wl["expect"]).all() and (b == a).all()
+    assert ctx.register_pk_affine_batch(np.zeros((0, 24), dtype=np.uint64)).size == 0
