@@ -165,6 +165,36 @@ def cpu_rate(C, wl, g2, count, threads):
     return count / dt, dt
 
 
+# The reference's own CPU figure for one verification (ic_bls12_381 0.10.1 on
+# the authors' CPU, not named; cuda/bench_bls_verify.cu:167,228): context for
+# reading the port's rate, not a measurement on this host.
+REF_CPU_US_PER_VERIFY = 348.0
+
+
+def host_cores():
+    """(physical cores, logical CPUs) of this host"""
+    logical = os.cpu_count() or 1
+    try:
+        import psutil
+        phys = psutil.cpu_count(logical=False) or logical
+    except Exception:
+        phys = logical
+    return phys, logical
+
+
+def cpu_context(rate, threads):
+    """what a reader needs to place the CPU rate: cores, threads, time per
+    verification per thread, and the reference's own single-thread figure"""
+    phys, logical = host_cores()
+    us = 1e6 * threads / rate
+    return {"physical_cores": phys, "logical_cpus": logical, "threads": threads,
+            "us_per_verify_per_thread": round(us, 1),
+            "reference_us_per_verify": REF_CPU_US_PER_VERIFY,
+            "reference_us_basis": "ic_bls12_381 0.10.1 single verify on the reference authors' CPU "
+                                  "(cuda/bench_bls_verify.cu:167,228), not measured here",
+            "rate_at_reference_speed": round(threads * 1e6 / REF_CPU_US_PER_VERIFY, 1)}
+
+
 def cpu_baseline(wl, g2, target_s=12.0):
     C = cpu_verifier()
     threads = C.num_threads()
@@ -174,7 +204,8 @@ def cpu_baseline(wl, g2, target_s=12.0):
     rate, dt = cpu_rate(C, wl, g2, count, threads)
     return {"value": rate, "unit": "verifies/s", "cores": threads, "kind": "port",
             "sample": "%d items cycling through the %d-item workload, oracle/cpu_verifier.cpp on %d host "
-                      "threads, %.1f s" % (count, N_ITEMS, threads, dt)}
+                      "threads, %.1f s" % (count, N_ITEMS, threads, dt),
+            **cpu_context(rate, threads)}
 
 
 def run_reference(args):
@@ -203,7 +234,8 @@ def run_reference(args):
         "config": {"workload": "keyset-4096-40: 4,096 verifications over 40 public keys",
                    "step_sample": per_step, "l2": "n/a (CPU)"},
         "cpu_baseline": {"value": value, "unit": "verifies/s", "cores": threads, "kind": "port",
-                         "sample": "%d items per step, cycling through the 4,096-item workload" % per_step},
+                         "sample": "%d items per step, cycling through the 4,096-item workload" % per_step,
+                         **cpu_context(value, threads)},
         "e2e": {"value": value, "unit": "verifies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CPU verifier = oracle/cpu_verifier.cpp (restatement of ic_bls12_381's verify as the "
                 "reference's GPU code mirrors it); the reference's Rust crates are not buildable offline",
@@ -240,7 +272,9 @@ def run_gpu(args):
 
     wl = WL.config_keyset(N_ITEMS, N_KEYS, seed=SEED + rank)
     ctx = G.Context(device=local, lanes=args.lanes)
-    ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
+    t_keys = time.perf_counter()
+    ids = ctx.register_pk_affine_batch(wl["pk_affine"])
+    key_setup_ms = 1e3 * (time.perf_counter() - t_keys)
     for i in (0, N_KEYS - 1):  # device tables == caller-built tables
         assert (ctx.pk_table(int(ids[i])) == wl["pk_tables"][i]).all()
     pk_ids = ids[wl["pk_index"]]
@@ -356,9 +390,9 @@ def run_gpu(args):
         roofline = {
             "bound": "int32-imad", "achieved": round(achieved_timad, 3), "peak": round(peak_timad, 3),
             "unit": "TIMAD/s", "frac": round(achieved_timad / peak_timad, 4), "traffic": DRAM_BYTES_PER_LAUNCH,
-            "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-verify launch, ncu "
-                             "capture summarised in profiles/k_verify_fp2_keyset4096.md (line tables and points; "
-                             "the bound is the IMAD pipe, not DRAM)",
+            "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-verify launch from an "
+                             "ncu capture of this kernel (line tables and points; the bound is the IMAD pipe, "
+                             "not DRAM)",
             "peak_basis": "%d SMs x 64 IMAD/clk x %.0f MHz (median SM clock sampled during the timed region)"
                           % (sms, clk),
             "algorithmic_imad_per_verify": ALGO_IMAD_PER_VERIFY,
@@ -388,6 +422,8 @@ def run_gpu(args):
             "clocks": clocks,
             "gpu_launches": args.steps,
             "bit_exact": True,
+            "key_setup": {"keys": N_KEYS, "api": "bls_pk_register_affine_batch (line tables and their "
+                          "normalisation for every key, one launch each)", "ms": round(key_setup_ms, 2)},
         }
         if ref_abi:
             result["e2e"]["reference_abi"] = ref_abi

@@ -8,14 +8,16 @@ This script reads those files as text, by file and line range, and stores the
 once in a container that has the reference checked out; the JSON it writes is
 the committed fixture, so nothing at test time needs the reference.
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT (the reference's checkout)")
+REF = sys.argv[1]
 HEX_C = re.compile(r"0x([0-9a-fA-F]+)(?:ULL|ull)?")
 
 
