@@ -271,7 +271,7 @@ def run_gpu(args):
         pg = dist
 
     wl = WL.config_keyset(N_ITEMS, N_KEYS, seed=SEED + rank)
-    ctx = G.Context(device=local, lanes=args.lanes)
+    ctx = G.Context(device=local, lanes=args.lanes, threads_per_block=args.threads_per_block)
     t_keys = time.perf_counter()
     ids = ctx.register_pk_affine_batch(wl["pk_affine"])
     key_setup_ms = 1e3 * (time.perf_counter() - t_keys)
@@ -398,7 +398,8 @@ def run_gpu(args):
             "algorithmic_imad_per_verify": ALGO_IMAD_PER_VERIFY,
             "own_imad_per_verify": IMAD_PER_VERIFY, "own_products_per_verify": OWN_PRODUCTS_PER_VERIFY,
             "own_reductions_per_verify": OWN_REDC_PER_VERIFY,
-            "kernel": ("k_verify_fp2" if args.lanes == 6 else "k_verify_lanes<%d>" % args.lanes) if args.lanes > 1
+            "kernel": (("k_verify_fp2" if args.threads_per_block == 64 else "k_verify_w") if args.lanes == 6
+                       else "k_verify_lanes<%d>" % args.lanes) if args.lanes > 1
             else "k_verify",
             "kernel_ms": round(kernel_ms, 4),
             "chain_ceiling": round(chain_timad, 3),
@@ -507,49 +508,55 @@ def run_compressed(G, WL, ctx, n=65536, reps=3):
 
 
 def run_batching(G, WL, ctx, wl_headline, reps=2):
-    """Batching workload: 256 requests, sizes log-uniform in [1, 2048], 1-40 keys each;
+    """Batching workload: 256 requests, sizes log-uniform in [1, 2048], 1-40 keys each.
+    First the autotuner (bls_autotune: lanes per verification x block shape x
+    blocks per SM) on a device-resident 16,384-item slice of this mix, in a
+    context of its own that keeps the fastest point; then, with that point,
     one launch per request against one persistent graph-replayed launch, both
-    through bls_verify_requests from host buffers (host-timed, best of reps).
-    Then the autotuner's sweep (bls_autotune: lanes per verification x blocks
-    per SM, each timed on the headline workload resident on the device) on a
-    context of its own, since the sweep keeps its choice in the context."""
-    wl = WL.config_requests(256, 2048, N_KEYS, seed=4)
-    ids = np.array([ctx.register_pk_affine(q) for q in wl["pk_affine"]], dtype=np.int32)
-    off = wl["offsets"]
-    reqs = [(wl["sigs"][a:b], wl["nhms"][a:b], ids[wl["pk_index"][a:b]]) for a, b in zip(off[:-1], off[1:])]
-    n = int(off[-1])
-    out = {"requests": len(reqs), "items": n, "sizes": "log-uniform [1, 2048]"}
-    for mode, name in ((G.MODE_PLAIN, "plain"), (G.MODE_PERSISTENT, "persistent")):
-        r = ctx.verify_requests(reqs, mode=mode)
-        assert (np.concatenate(r) == wl["expect"]).all(), "batched accept bits differ"
-        best = 1e30
-        for _ in range(reps):
-            t0 = time.perf_counter()
-            ctx.verify_requests(reqs, mode=mode)
-            best = min(best, time.perf_counter() - t0)
-        out[name + "_verifies_per_s"] = round(n / best, 1)
-        out[name + "_ms"] = round(best * 1e3, 2)
-    out["speedup"] = round(out["persistent_verifies_per_s"] / out["plain_verifies_per_s"], 2)
-
+    through bls_verify_requests from host buffers (host-timed, best of reps)."""
     import torch
-    tctx = G.Context()
+    wl = WL.config_requests(256, 2048, N_KEYS, seed=4)
+    bctx = G.Context()
     try:
-        tids = np.array([tctx.register_pk_affine(q) for q in wl_headline["pk_affine"]],
-                        dtype=np.int32)[wl_headline["pk_index"]]
+        ids = bctx.register_pk_affine_batch(wl["pk_affine"])
+        m = min(16384, len(wl["expect"]))
         dev = torch.device("cuda", torch.cuda.current_device())
-        ds = torch.from_numpy(wl_headline["sigs"].view(np.int64)).to(dev)
-        dn = torch.from_numpy(wl_headline["nhms"].view(np.int64)).to(dev)
-        di = torch.from_numpy(tids).to(dev)
-        pts = tctx.autotune(len(tids), ds.data_ptr(), dn.data_ptr(), di.data_ptr(), repeats=2)
+        ds = torch.from_numpy(wl["sigs"][:m].view(np.int64)).to(dev)
+        dn = torch.from_numpy(wl["nhms"][:m].view(np.int64)).to(dev)
+        di = torch.from_numpy(ids[wl["pk_index"][:m]]).to(dev)
+        pts = bctx.autotune(m, ds.data_ptr(), dn.data_ptr(), di.data_ptr(), repeats=2)
+        off = wl["offsets"]
+        reqs = [(wl["sigs"][a:b], wl["nhms"][a:b], ids[wl["pk_index"][a:b]]) for a, b in zip(off[:-1], off[1:])]
+        n = int(off[-1])
+        out = {"requests": len(reqs), "items": n, "sizes": "log-uniform [1, 2048]"}
+        for mode, name in ((G.MODE_PLAIN, "plain"), (G.MODE_PERSISTENT, "persistent")):
+            r = bctx.verify_requests(reqs, mode=mode)
+            assert (np.concatenate(r) == wl["expect"]).all(), "batched accept bits differ"
+            best = 1e30
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                bctx.verify_requests(reqs, mode=mode)
+                best = min(best, time.perf_counter() - t0)
+            out[name + "_verifies_per_s"] = round(n / best, 1)
+            out[name + "_ms"] = round(best * 1e3, 2)
+        out["speedup"] = round(out["persistent_verifies_per_s"] / out["plain_verifies_per_s"], 2)
     finally:
-        tctx.close()
-    lanes_name = {1: "thread per verification", 6: "Fp2 lanes (12 threads)"}
-    best = min(pts, key=lambda p: p[2])
+        bctx.close()
+    kernel = {1: "k_verify (thread per verification)", 2: "k_verify_lanes<2>", 4: "k_verify_lanes<4>",
+              8: "k_verify_lanes<8>"}
+
+    def name(l, tpb):
+        if l == 6:
+            return "k_verify_w (32 items / 12 warps)" if tpb == 384 else "k_verify_fp2 (5 items / 2 warps)"
+        return kernel.get(l, "%d lanes" % l)
+    best = min(pts, key=lambda p: p[3])
     out["autotune"] = {
-        "sample": "keyset-4096-40, inputs resident (bls_autotune, best of 2 per point)",
-        "points": [{"lanes": l, "kernel": lanes_name.get(l, "%d lanes" % l), "blocks_per_sm": b, "ms": round(ms, 3)}
-                   for l, b, ms in pts],
-        "chosen": {"lanes": best[0], "blocks_per_sm": best[1], "ms": round(best[2], 3)}}
+        "sample": "first %d items of this mix (mixed keys), inputs resident (bls_autotune, best of 2 per point); "
+                  "the chosen point runs both request modes above" % m,
+        "points": [{"lanes": l, "threads_per_block": t, "kernel": name(l, t), "blocks_per_sm": b, "ms": round(ms, 3)}
+                   for l, t, b, ms in pts],
+        "chosen": {"lanes": best[0], "threads_per_block": best[1], "kernel": name(best[0], best[1]),
+                   "blocks_per_sm": best[2], "ms": round(best[3], 3)}}
     return out
 
 
@@ -740,6 +747,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batching and serving sections")
     ap.add_argument("--lanes", type=int, default=6, help="lanes per verification (6: Fp2-lane kernel; 1, 2, 4, 8)")
+    ap.add_argument("--threads-per-block", type=int, default=0,
+                    help="six lanes: 384 (32 items per block, twelve warps; the default), 64 (five items, two warps)")
     ap.add_argument("--ingest-keys", default="1024,16384",
                     help="comma-separated key counts ingested compressed on the GPU (0 = skip)")
     ap.add_argument("--rlc-items", type=int, default=65536, help="random-linear-combination batch draw (0 = skip)")

@@ -54,7 +54,8 @@ class Request(ctypes.Structure):
 
 
 class TunePoint(ctypes.Structure):
-    _fields_ = [("lanes_per_pairing", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("ms", ctypes.c_float)]
+    _fields_ = [("lanes_per_pairing", ctypes.c_int), ("threads_per_block", ctypes.c_int),
+                ("blocks_per_sm", ctypes.c_int), ("ms", ctypes.c_float)]
 
 
 MODE_PLAIN, MODE_PERSISTENT = 0, 1
@@ -222,7 +223,8 @@ def verify_compressed_noalloc(sigs48_ptr, nhms_ptr, g2_ptr, pk_tables_ptr, pk_id
 class Context:
     """A device context: stream, buffers and resident public-key tables."""
 
-    def __init__(self, device=0, max_batch=0, max_pks=0, mem_cap_bytes=0, lanes=0, blocks_per_sm=0):
+    def __init__(self, device=0, max_batch=0, max_pks=0, mem_cap_bytes=0, lanes=0, blocks_per_sm=0,
+                 threads_per_block=0):
         L = lib()
         cfg = Config()
         L.bls_config_default(ctypes.byref(cfg), device)
@@ -233,6 +235,7 @@ class Context:
         cfg.mem_cap_bytes = mem_cap_bytes
         cfg.lanes_per_pairing = lanes
         cfg.blocks_per_sm = blocks_per_sm
+        cfg.threads_per_block = threads_per_block
         h = ctypes.c_void_p()
         rc = L.bls_ctx_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != BLS_OK:
@@ -426,13 +429,14 @@ class Context:
 
     def autotune(self, n, sigs_ptr, nhms_ptr, ids_ptr, compressed=False, repeats=3):
         """Time every kernel configuration on a device-resident sample and keep
-        the fastest; returns [(lanes, blocks_per_sm, ms), ...]."""
+        the fastest; returns [(lanes, threads_per_block, blocks_per_sm, ms), ...]."""
         b = Batch(n, SIG_COMPRESSED if compressed else SIG_AFFINE, sigs_ptr, nhms_ptr, ids_ptr, None, None)
         pts = (TunePoint * 32)()
         npts = ctypes.c_int()
         self._check(self.lib.bls_autotune(self.h, ctypes.byref(b), repeats, pts, 32, ctypes.byref(npts)),
                     "bls_autotune")
-        return [(pts[i].lanes_per_pairing, pts[i].blocks_per_sm, pts[i].ms) for i in range(npts.value)]
+        return [(pts[i].lanes_per_pairing, pts[i].threads_per_block, pts[i].blocks_per_sm, pts[i].ms)
+                for i in range(npts.value)]
 
 
 class Server:

@@ -249,6 +249,9 @@ int ctx_init(bls_ctx* c, const bls_config* cfg) {
     int l = c->cfg.lanes_per_pairing;
     if (l != 1 && l != 2 && l != 4 && l != 6 && l != 8)
         return fail(BLS_ERR_INVALID, "lanes_per_pairing must be 1, 2, 4, 6 or 8 (got %d)", l);
+    const int tpb = c->cfg.threads_per_block;
+    if (tpb != 0 && !(l == 6 && (tpb == bls::kShapeFive || tpb == bls::kShapeWide)))
+        return fail(BLS_ERR_INVALID, "threads_per_block must be 0, or 64 or 384 with six lanes (got %d)", tpb);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return fail(BLS_ERR_NODEV, "no CUDA device");
@@ -326,7 +329,8 @@ int run_verify(bls_ctx* c, bls::VerifyArgs a) {
         status = (const uint32_t*)c->d_st.p;
     }
     if (a.work_counter) CK(cudaMemsetAsync(a.work_counter, 0, sizeof(int), c->stream));
-    CK(bls::launch_verify_lanes(a, status, c->cfg.lanes_per_pairing, c->cfg.blocks_per_sm, c->sms, c->stream));
+    CK(bls::launch_verify_lanes(a, status, c->cfg.lanes_per_pairing, c->cfg.threads_per_block, c->cfg.blocks_per_sm,
+                                c->sms, c->stream));
     return BLS_OK;
 }
 
@@ -414,7 +418,8 @@ CtxView ctx_view(bls_ctx* c) {
     std::lock_guard<std::mutex> lk(c->mu);
     bls::VerifyArgs a{};
     c->set_norm(a);
-    return CtxView{c->cfg.device, c->sms, c->cfg.lanes_per_pairing, c->cfg.blocks_per_sm,
+    return CtxView{c->cfg.device, c->sms, c->cfg.lanes_per_pairing, bls::six_lane_shape(c->cfg.threads_per_block),
+                   c->cfg.blocks_per_sm,
                    c->d_g2, c->d_pk, c->d_pk_inf, c->n_pks, a.g2_norm, a.pk_norm, a.g2_corr, a.pk_corr};
 }
 }  // namespace bls
@@ -798,12 +803,14 @@ int bls_verify_requests(bls_ctx* ctx, const bls_request* reqs, int nreq, int fmt
     }
     std::vector<const void*> key = {(const void*)total, (const void*)(size_t)fmt,
                                     (const void*)(size_t)ctx->cfg.lanes_per_pairing,
+                                    (const void*)(size_t)ctx->cfg.threads_per_block,
                                     (const void*)(size_t)ctx->cfg.blocks_per_sm, ctx->d_sigs.p, ctx->d_nhms.p,
                                     ctx->d_pkidx.p, ctx->d_res.p, ctx->d_work.p, ctx->d_xy.p, ctx->d_st.p,
                                     ctx->h_sigs.p, ctx->h_nhms.p, ctx->h_pkidx.p, ctx->h_res.p};
     if (!ctx->graph || ctx->graph_key != key) {
         ctx->drop_graph();
-        if (ctx->cfg.lanes_per_pairing > 1) bls::verify_lanes_blocks_per_sm(ctx->cfg.lanes_per_pairing);  // set up outside capture
+        if (ctx->cfg.lanes_per_pairing > 1)   // set up outside capture
+            bls::verify_lanes_blocks_per_sm(ctx->cfg.lanes_per_pairing, ctx->cfg.threads_per_block);
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         rc = enqueue(ctx, total, fmt, true, false, false);
@@ -852,24 +859,29 @@ int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* 
     if (b->sig_format == BLS_SIG_COMPRESSED &&
         ((rc = ctx->grow(ctx->d_xy, (size_t)b->n * 96)) || (rc = ctx->grow(ctx->d_st, (size_t)b->n * 4))))
         return rc;
-    struct Cand { int lanes, bps; };
+    // candidates: lanes per verification x block shape (six lanes: five items
+    // in two warps or 32 items in twelve warps) x resident blocks per SM
+    struct Cand { int lanes, tpb, bps; };
     std::vector<Cand> cands;
-    cands.push_back({1, 0});
+    cands.push_back({1, 0, 0});
     for (int l : {2, 4, 6, 8}) {
-        int res = bls::verify_lanes_blocks_per_sm(l);
-        cands.push_back({l, 0});
-        for (int bps : {res - 1, res / 2})
-            if (bps >= 1 && bps < res) cands.push_back({l, bps});
+        for (int tpb : l == 6 ? std::vector<int>{bls::kShapeWide, bls::kShapeFive} : std::vector<int>{0}) {
+            int res = bls::verify_lanes_blocks_per_sm(l, tpb);
+            cands.push_back({l, tpb, 0});
+            for (int bps : {res - 1, res / 2})
+                if (bps >= 1 && bps < res) cands.push_back({l, tpb, bps});
+        }
     }
     bls_config saved = ctx->cfg;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
-    Cand bestc = {saved.lanes_per_pairing, saved.blocks_per_sm};
+    Cand bestc = {saved.lanes_per_pairing, saved.threads_per_block, saved.blocks_per_sm};
     int np = 0;
     for (const Cand& cd : cands) {
         ctx->cfg.lanes_per_pairing = cd.lanes;
+        ctx->cfg.threads_per_block = cd.tpb;
         ctx->cfg.blocks_per_sm = cd.bps;
         bls::VerifyArgs a{};
         a.sigs = b->sigs;
@@ -895,7 +907,8 @@ int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* 
             if (ms < ms_best) ms_best = ms;
         }
         if (rc) break;
-        if (points && np < max_points) points[np] = {cd.lanes, cd.bps, ms_best};
+        if (points && np < max_points) points[np] = {cd.lanes, cd.tpb ? cd.tpb : (cd.lanes == 6 ? bls::six_lane_shape(0) : 0),
+                                                     cd.bps, ms_best};
         ++np;
         if (ms_best < best) {
             best = ms_best;
@@ -907,6 +920,7 @@ int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* 
     ctx->cfg = saved;
     if (rc) return rc;
     ctx->cfg.lanes_per_pairing = bestc.lanes;
+    ctx->cfg.threads_per_block = bestc.tpb;
     ctx->cfg.blocks_per_sm = bestc.bps;
     ctx->drop_graph();
     if (n_points) *n_points = np < max_points ? np : max_points;

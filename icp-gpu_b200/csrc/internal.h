@@ -78,24 +78,39 @@ cudaError_t launch_g2_prepare(const uint64_t* q, int n, uint64_t* out, cudaStrea
 // correction factor (12 u64) and a flag set when a c2 is zero (table copied)
 cudaError_t launch_lines_normalize(const uint64_t* raw, int n, uint64_t* norm, uint64_t* corr, uint8_t* bad,
                                    cudaStream_t s);
+// Block shapes of the six-lane (Fp2-lane) kernels, by threads per block:
+// kShapeFive (64 threads, two warps, five items per block: k_verify_fp2) and
+// kShapeWide (384 threads, twelve warps, 32 items per block, one per lane:
+// k_verify_w).  0 selects kDefaultShape.
+constexpr int kShapeFive = 64, kShapeWide = 384;
+constexpr int kDefaultShape = kShapeWide;
+inline int six_lane_shape(int threads_per_block) { return threads_per_block > 0 ? threads_per_block : kDefaultShape; }
+
 // lane-parallel verify; in_status: per-item decode status or NULL.  lanes 6
-// runs the Fp2-lane kernel (verify_fp2.cu), 2, 4 and 8 the interpreter of
-// per-Fp programs (verify_vm.cu).
-cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int blocks_per_sm,
-                                int sms, cudaStream_t s);
-cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks, int sms, cudaStream_t s);
+// runs an Fp2-lane kernel of block shape `shape` (verify_fp2.cu or
+// verify_w.cu), 2, 4 and 8 the interpreter of per-Fp programs (verify_vm.cu).
+cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int shape,
+                                int blocks_per_sm, int sms, cudaStream_t s);
+cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, const uint32_t* in_status, int blocks, int sms,
+                                   cudaStream_t s);
 cudaError_t launch_verify_fp2(const VerifyArgs& a, const uint32_t* in_status, int blocks_per_sm, int sms,
                               cudaStream_t s);
 size_t verify_fp2_smem_bytes();
 int verify_fp2_blocks_per_sm();
+// the twelve-warp form: one block per SM; ring serving claims up to 32 items
+cudaError_t launch_verify_w(const VerifyArgs& a, const uint32_t* in_status, int sms, cudaStream_t s);
+cudaError_t launch_verify_w_serve(const VerifyArgs& a, const uint32_t* in_status, int blocks, int sms,
+                                 cudaStream_t s);
+size_t verify_w_smem_bytes();
+int verify_w_blocks_per_sm();
 cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s, double* imad_per_s);
-size_t verify_lanes_smem_bytes(int lanes);
+size_t verify_lanes_smem_bytes(int lanes, int shape = 0);
 // blocks of the lane-parallel kernel resident per SM (occupancy calculator)
-int verify_lanes_blocks_per_sm(int lanes);
+int verify_lanes_blocks_per_sm(int lanes, int shape = 0);
 
 // what the serving loop (server.cpp) needs from a context
 struct CtxView {
-    int device, sms, lanes, blocks_per_sm;
+    int device, sms, lanes, shape, blocks_per_sm;
     const uint64_t* g2;
     const uint64_t* pk_tables;
     const uint8_t* pk_identity;

@@ -120,7 +120,7 @@ extern "C" int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64
     a.n = n;
     a.results = results;
     a.work_counter = counter;
-    if (bls::launch_verify_lanes(a, reinterpret_cast<const uint32_t*>(status), lanes_per_pairing, 0, sms, s) !=
+    if (bls::launch_verify_lanes(a, reinterpret_cast<const uint32_t*>(status), lanes_per_pairing, 0, 0, sms, s) !=
         cudaSuccess)
         return BLS_ERR_CUDA;
     return BLS_OK;

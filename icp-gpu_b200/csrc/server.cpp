@@ -19,17 +19,19 @@
 // to what the budget admits.  Waits are bounded (timeouts), the dispatcher
 // never spins on the device: it sleeps on a condition variable between polls.
 //
-// Ring mode (BLS_SERVE_RING): requests are padded to whole groups of five
-// with identity items and written into host mirrors of a device ring of item
-// slots; one copy stream moves each new range (inputs and sentinel results) to
-// the device and then raises the published-item count in device memory.  One
-// persistent launch of the six-lane kernel claims published groups from a
-// device counter as blocks free up and writes each result into the ring.  The
-// dispatcher copies the results of the in-flight range back, sees a request
-// complete when none of its result slots holds the sentinel any more, copies
-// its results out and frees ring space in order.  Admission is by ring space.
-// The kernel leaves when idle for 20 ms, on destroy, or 60 s after its launch;
-// the dispatcher relaunches it while work is left.
+// Ring mode (BLS_SERVE_RING): requests are written into host mirrors of a
+// device ring of item slots (padded with identity items to whole groups of
+// five for the five-item block shape; the twelve-warp shape claims any count
+// up to 32, so nothing is padded); one copy stream moves each new range
+// (inputs and sentinel results) to the device and then raises the
+// published-item count in device memory.  One persistent launch of the
+// six-lane kernel claims published items from a device counter as blocks
+// free up and writes each result into the ring.  The dispatcher copies the
+// results of the in-flight range back, sees a request complete when none of
+// its result slots holds the sentinel any more, copies its results out and
+// frees ring space in order.  Admission is by ring space.  The kernel leaves
+// when idle for 20 ms, on destroy, or 60 s after its launch; the dispatcher
+// relaunches it while work is left.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -80,10 +82,16 @@ struct Slot {
 
 // ring mode state: device ring and its host mirrors (same slot indexing)
 struct Ring {
-    uint32_t cap = 0;                      // item slots, a multiple of 5
+    uint32_t cap = 0;                      // item slots, a multiple of `group`
+    uint32_t group = 1;                    // claim granule: 5 (five-item blocks, requests padded) or 1
     uint64_t *h_sigs = nullptr, *h_nhms = nullptr;   // pinned mirrors: cap x 12
     int32_t *h_ids = nullptr, *h_res = nullptr;      // cap
     uint32_t* h_ctl = nullptr;             // pinned: [0] published items, [1] stop
+    // compressed signatures: 48-byte encodings in (pinned mirror and device),
+    // decoded into d_sigs with a per-slot status by the decoder on the copy
+    // stream before the range is published
+    uint8_t *h_comp = nullptr, *d_comp = nullptr;
+    int32_t* d_st = nullptr;
     uint64_t *d_sigs = nullptr, *d_nhms = nullptr;
     int32_t *d_ids = nullptr, *d_res = nullptr;
     uint32_t* d_ctl = nullptr;             // device: [0] published, [1] stop, [2] claimed
@@ -99,7 +107,9 @@ struct Ring {
     std::deque<Flight> flights;
 };
 constexpr int32_t kSentinel = 0x7fffffff;
-constexpr uint32_t kGroup = 5;
+// SMs left free of the twelve-warp ring kernel for the decoder of compressed
+// signatures (a block of the decoder does not fit beside a resident block)
+constexpr int kDecodeSms = 4;
 
 struct bls_server {
     bls_ctx* ctx = nullptr;
@@ -156,7 +166,7 @@ struct bls_server {
             status = (const uint32_t*)s.d_st;
         }
         int lanes = view.lanes > 1 ? view.lanes : 6;
-        if (bls::launch_verify_lanes(a, status, lanes, view.blocks_per_sm, view.sms, st) ||
+        if (bls::launch_verify_lanes(a, status, lanes, view.shape, view.blocks_per_sm, view.sms, st) ||
             cudaMemcpyAsync(s.h_res, s.d_res, n * 4, cudaMemcpyDeviceToHost, st) || cudaEventRecord(s.done, st))
             return BLS_ERR_CUDA;
         s.busy = true;
@@ -182,6 +192,7 @@ struct bls_server {
     int ring_launch() {
         bls::VerifyArgs a{};
         a.sigs = ring.d_sigs;
+        if (ring.d_comp) a.sig_xy = ring.d_sigs;   // decoded by the dispatcher's decoder
         a.nhms = ring.d_nhms;
         a.g2 = view.g2;
         a.pk_tables = view.pk_tables;
@@ -199,10 +210,16 @@ struct bls_server {
         a.serve_cap = ring.cap;
         a.serve_idle_ns = 20ull * 1000 * 1000;
         a.serve_max_ns = 60ull * 1000 * 1000 * 1000;
-        const int blocks = cfg.ring_blocks > 0 ? cfg.ring_blocks : cfg.ring_blocks_per_sm * view.sms;
-        if (bls::launch_verify_fp2_serve(a, blocks, view.sms, ring.kern) ||
-            cudaEventRecord(ring.done, ring.kern))
-            return BLS_ERR_CUDA;
+        int blocks = cfg.ring_blocks > 0 ? cfg.ring_blocks : cfg.ring_blocks_per_sm * view.sms;
+        // the twelve-warp kernel fills its SMs: with compressed signatures a few
+        // SMs stay free for the decoder, which runs beside the resident kernel
+        if (ring.d_comp && view.shape == bls::kShapeWide && blocks > view.sms - kDecodeSms)
+            blocks = view.sms - kDecodeSms;
+        const uint32_t* st = (const uint32_t*)ring.d_st;
+        const cudaError_t e = view.shape == bls::kShapeWide
+                                  ? bls::launch_verify_w_serve(a, st, blocks, view.sms, ring.kern)
+                                  : bls::launch_verify_fp2_serve(a, st, blocks, view.sms, ring.kern);
+        if (e != cudaSuccess || cudaEventRecord(ring.done, ring.kern) != cudaSuccess) return BLS_ERR_CUDA;
         ring.launched = true;
         return BLS_OK;
     }
@@ -215,6 +232,18 @@ struct bls_server {
                             ring.copy))
             return BLS_ERR_CUDA;
         if (first < n && cudaMemcpyAsync(dst, src, sizeof(T) * per * (n - first), cudaMemcpyHostToDevice, ring.copy))
+            return BLS_ERR_CUDA;
+        return BLS_OK;
+    }
+
+    // decode ring range [a, a + n) (may wrap) on the copy stream: the decoded
+    // points into d_sigs, each slot's decode status into d_st
+    int ring_decode(uint32_t a, uint32_t n) {
+        const uint32_t s0 = a % ring.cap, first = std::min(n, ring.cap - s0);
+        if (bls::launch_g1_decompress(ring.d_comp + 48 * (size_t)s0, (int)first, ring.d_sigs + 12 * (size_t)s0,
+                                      ring.d_st + s0, ring.copy))
+            return BLS_ERR_CUDA;
+        if (first < n && bls::launch_g1_decompress(ring.d_comp, (int)(n - first), ring.d_sigs, ring.d_st, ring.copy))
             return BLS_ERR_CUDA;
         return BLS_OK;
     }
@@ -267,7 +296,7 @@ struct bls_server {
         for (uint64_t tk : finished) done[tk] = t;
         items += finished_items;
         while (!queue.empty()) {
-            const uint32_t span = ((uint32_t)queue.front().n + kGroup - 1) / kGroup * kGroup;
+            const uint32_t span = ((uint32_t)queue.front().n + ring.group - 1) / ring.group * ring.group;
             if (span > room) break;
             room -= span;
             if ((uint64_t)queue.front().n > max_batch) max_batch = queue.front().n;
@@ -281,16 +310,24 @@ struct bls_server {
         }
         const uint32_t from = ring.pub;
         for (Pending& q : admit) {
-            const uint32_t span = ((uint32_t)q.n + kGroup - 1) / kGroup * kGroup;
+            const uint32_t span = ((uint32_t)q.n + ring.group - 1) / ring.group * ring.group;
             for (uint32_t k = 0; k < span; ++k) {
                 const uint32_t slot = (ring.pub + k) % ring.cap;
                 ring.h_res[slot] = kSentinel;
                 if (k < (uint32_t)q.n) {
-                    memcpy(ring.h_sigs + 12 * (size_t)slot, q.sigs.data() + 96 * (size_t)k, 96);
+                    if (ring.h_comp)
+                        memcpy(ring.h_comp + 48 * (size_t)slot, q.sigs.data() + 48 * (size_t)k, 48);
+                    else
+                        memcpy(ring.h_sigs + 12 * (size_t)slot, q.sigs.data() + 96 * (size_t)k, 96);
                     memcpy(ring.h_nhms + 12 * (size_t)slot, q.nhms.data() + 12 * (size_t)k, 96);
                     ring.h_ids[slot] = q.ids[k];
                 } else {  // padding: identity points, key 0 (both pairs skipped)
-                    memset(ring.h_sigs + 12 * (size_t)slot, 0, 96);
+                    if (ring.h_comp) {
+                        memset(ring.h_comp + 48 * (size_t)slot, 0, 48);
+                        ring.h_comp[48 * (size_t)slot] = 0xc0;   // the identity's encoding
+                    } else {
+                        memset(ring.h_sigs + 12 * (size_t)slot, 0, 96);
+                    }
                     memset(ring.h_nhms + 12 * (size_t)slot, 0, 96);
                     ring.h_ids[slot] = 0;
                 }
@@ -301,7 +338,8 @@ struct bls_server {
         int rc = BLS_OK;
         if (ring.pub != from) {
             const uint32_t n = ring.pub - from;
-            if ((rc = ring_copy_in(ring.d_sigs, ring.h_sigs, 12, from, n)) ||
+            if ((ring.h_comp ? (rc = ring_copy_in(ring.d_comp, ring.h_comp, 48, from, n)) || (rc = ring_decode(from, n))
+                             : (rc = ring_copy_in(ring.d_sigs, ring.h_sigs, 12, from, n))) ||
                 (rc = ring_copy_in(ring.d_nhms, ring.h_nhms, 12, from, n)) ||
                 (rc = ring_copy_in(ring.d_ids, ring.h_ids, 1, from, n)) ||
                 (rc = ring_copy_in(ring.d_res, ring.h_res, 1, from, n))) {
@@ -413,7 +451,7 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
     if (s->cfg.mem_cap_bytes == 0) s->cfg.mem_cap_bytes = (size_t)4 << 30;
     if ((s->cfg.sig_format != BLS_SIG_AFFINE && s->cfg.sig_format != BLS_SIG_COMPRESSED) ||
         (s->cfg.mode != BLS_SERVE_SLOTS && s->cfg.mode != BLS_SERVE_RING) ||
-        (s->cfg.mode == BLS_SERVE_RING && s->cfg.sig_format != BLS_SIG_AFFINE) || s->cfg.ring_items < 0 ||
+        s->cfg.ring_items < 0 ||
         s->cfg.ring_blocks_per_sm < 0 || s->cfg.ring_blocks < 0) {
         delete s;
         return BLS_ERR_INVALID;
@@ -429,14 +467,18 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
             return BLS_ERR_INVALID;
         }
         Ring& r = s->ring;
-        if (s->cfg.ring_blocks_per_sm == 0) s->cfg.ring_blocks_per_sm = 4;
-        const int most = bls::verify_lanes_blocks_per_sm(6);
+        // resident blocks: the twelve-warp kernel holds a whole SM per block; the
+        // five-item kernel defaults to 4 of its 6 blocks per SM (the latency choice)
+        if (s->cfg.ring_blocks_per_sm == 0) s->cfg.ring_blocks_per_sm = s->view.shape == bls::kShapeWide ? 1 : 4;
+        const int most = bls::verify_lanes_blocks_per_sm(6, s->view.shape);
         if (most > 0 && s->cfg.ring_blocks_per_sm > most) s->cfg.ring_blocks_per_sm = most;
         uint64_t cap = s->cfg.ring_items > 0 ? (uint64_t)s->cfg.ring_items : 65535u;
-        const uint64_t least = (uint64_t)s->cfg.max_batch_items + 2 * kGroup;
+        r.group = s->view.shape == bls::kShapeWide ? 1u : 5u;
+        const uint64_t least = (uint64_t)s->cfg.max_batch_items + 2 * r.group;
         if (cap < least) cap = least;
-        cap = (cap + kGroup - 1) / kGroup * kGroup;
-        if (cap * 200 + 64 > s->cfg.mem_cap_bytes || cap > (1u << 30)) {
+        cap = (cap + r.group - 1) / r.group * r.group;
+        const bool comp = s->cfg.sig_format == BLS_SIG_COMPRESSED;
+        if (cap * (comp ? 252 : 200) + 64 > s->cfg.mem_cap_bytes || cap > (1u << 30)) {
             delete s;
             return BLS_ERR_NOMEM;
         }
@@ -451,6 +493,9 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
                   cudaMalloc((void**)&r.d_ids, cap * 4) == cudaSuccess &&
                   cudaMalloc((void**)&r.d_res, cap * 4) == cudaSuccess &&
                   cudaMalloc((void**)&r.d_ctl, 64) == cudaSuccess && cudaMemset(r.d_ctl, 0, 64) == cudaSuccess &&
+                  (!comp || (cudaHostAlloc((void**)&r.h_comp, cap * 48, 0) == cudaSuccess &&
+                             cudaMalloc((void**)&r.d_comp, cap * 48) == cudaSuccess &&
+                             cudaMalloc((void**)&r.d_st, cap * 4) == cudaSuccess)) &&
                   cudaStreamCreateWithFlags(&r.copy, cudaStreamNonBlocking) == cudaSuccess &&
                   cudaStreamCreateWithFlags(&r.kern, cudaStreamNonBlocking) == cudaSuccess &&
                   cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming) == cudaSuccess &&
@@ -460,7 +505,7 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
             bls_server_destroy(s);
             return BLS_ERR_NOMEM;
         }
-        bls::verify_lanes_blocks_per_sm(6);
+        bls::verify_lanes_blocks_per_sm(6, s->view.shape);
         s->worker = std::thread([s] { s->run(); });
         *out = s;
         return BLS_OK;
@@ -489,7 +534,7 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
         }
     }
     // set up the kernel (shared-memory size, occupancy) before serving
-    bls::verify_lanes_blocks_per_sm(s->view.lanes > 1 ? s->view.lanes : 6);
+    bls::verify_lanes_blocks_per_sm(s->view.lanes > 1 ? s->view.lanes : 6, s->view.shape);
     s->worker = std::thread([s] { s->run(); });
     *out = s;
     return BLS_OK;
@@ -509,9 +554,11 @@ void bls_server_destroy(bls_server* s) {
     {
         Ring& r = s->ring;
         s->ring_stop();
-        for (void* p : {(void*)r.h_sigs, (void*)r.h_nhms, (void*)r.h_ids, (void*)r.h_res, (void*)r.h_ctl})
+        for (void* p : {(void*)r.h_sigs, (void*)r.h_nhms, (void*)r.h_ids, (void*)r.h_res, (void*)r.h_ctl,
+                        (void*)r.h_comp})
             if (p) cudaFreeHost(p);
-        for (void* p : {(void*)r.d_sigs, (void*)r.d_nhms, (void*)r.d_ids, (void*)r.d_res, (void*)r.d_ctl})
+        for (void* p : {(void*)r.d_sigs, (void*)r.d_nhms, (void*)r.d_ids, (void*)r.d_res, (void*)r.d_ctl,
+                        (void*)r.d_comp, (void*)r.d_st})
             if (p) cudaFree(p);
         if (r.done) cudaEventDestroy(r.done);
         if (r.copy) cudaStreamDestroy(r.copy);

@@ -618,7 +618,8 @@ cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s
 }
 
 // ring serving: `blocks` persistent blocks (at most the resident slots)
-cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks, int sms, cudaStream_t s) {
+cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, const uint32_t* in_status, int blocks, int sms,
+                                   cudaStream_t s) {
     if (!a.serve_avail || !a.serve_stop || !a.serve_claimed || a.serve_cap == 0 || a.serve_cap % kPairsPerBlock ||
         blocks <= 0)
         return cudaErrorInvalidValue;
@@ -626,7 +627,7 @@ cudaError_t launch_verify_fp2_serve(const VerifyArgs& a, int blocks, int sms, cu
     if (e != cudaSuccess) return e;
     const int res = resident();
     if (res > 0 && blocks > res * sms) blocks = res * sms;
-    k_verify_fp2<<<blocks, kThreads, smem_bytes(), s>>>(a, nullptr);
+    k_verify_fp2<<<blocks, kThreads, smem_bytes(), s>>>(a, in_status);
     return cudaGetLastError();
 }
 

@@ -329,18 +329,18 @@ cudaError_t launch_t(const VerifyArgs& a, const uint32_t* in_status, cudaStream_
 
 }  // namespace
 
-size_t verify_lanes_smem_bytes(int lanes) {
+size_t verify_lanes_smem_bytes(int lanes, int shape) {
     switch (lanes) {
-        case 6: return verify_fp2_smem_bytes();
+        case 6: return six_lane_shape(shape) == kShapeWide ? verify_w_smem_bytes() : verify_fp2_smem_bytes();
         case 2: return smem_t<2>();
         case 4: return smem_t<4>();
         default: return smem_t<8>();
     }
 }
 
-int verify_lanes_blocks_per_sm(int lanes) {
+int verify_lanes_blocks_per_sm(int lanes, int shape) {
     switch (lanes) {
-        case 6: return verify_fp2_blocks_per_sm();
+        case 6: return six_lane_shape(shape) == kShapeWide ? verify_w_blocks_per_sm() : verify_fp2_blocks_per_sm();
         case 2: return resident_t<2>();
         case 4: return resident_t<4>();
         case 8: return resident_t<8>();
@@ -348,11 +348,13 @@ int verify_lanes_blocks_per_sm(int lanes) {
     }
 }
 
-cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int blocks_per_sm,
-                                int sms, cudaStream_t s) {
+cudaError_t launch_verify_lanes(const VerifyArgs& a, const uint32_t* in_status, int lanes, int shape,
+                                int blocks_per_sm, int sms, cudaStream_t s) {
     if (a.n <= 0) return cudaSuccess;
     switch (lanes) {
-        case 6: return launch_verify_fp2(a, in_status, blocks_per_sm, sms, s);
+        case 6:
+            return six_lane_shape(shape) == kShapeWide ? launch_verify_w(a, in_status, sms, s)
+                                                       : launch_verify_fp2(a, in_status, blocks_per_sm, sms, s);
         case 2: return launch_t<2>(a, in_status, s, blocks_per_sm, sms);
         case 4: return launch_t<4>(a, in_status, s, blocks_per_sm, sms);
         case 8: return launch_t<8>(a, in_status, s, blocks_per_sm, sms);

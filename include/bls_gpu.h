@@ -112,7 +112,10 @@ typedef struct {
     int max_batch;          /* items per launch preallocated (grown on demand; 0 = 65536) */
     int max_pks;            /* public-key table slots (0 = 1024) */
     size_t mem_cap_bytes;   /* device-memory budget for this context (0 = none) */
-    int threads_per_block;  /* 0 = library default */
+    int threads_per_block;  /* block shape of the six-lane kernel: 0 = library default (384),
+                               384: twelve warps verify 32 items (one per lane, every warp
+                               one Fp2 coefficient and half), 64: two warps verify five
+                               items; must be 0 for other lane counts */
     int blocks_per_sm;      /* persistent launches: 0 = occupancy maximum */
     int lanes_per_pairing;  /* 6 (default, 0): six lanes per verification, one per Fp2
                                coefficient, lazy reduction (the fastest kernel);
@@ -200,13 +203,14 @@ int bls_verify_requests(bls_ctx* ctx, const bls_request* reqs, int nreq, int sig
 /* ---- autotuning ---- */
 typedef struct {
     int lanes_per_pairing;
+    int threads_per_block;      /* block shape (six lanes: 64 or 384; else 0) */
     int blocks_per_sm;          /* 0 = occupancy maximum */
     float ms;                   /* kernel time on the sample, best of the repeats */
 } bls_tune_point;
 
 /* Time the verify kernel on a device-resident sample batch for every
- * (lanes_per_pairing, blocks_per_sm) candidate, keep the fastest in the
- * context, and report up to max_points measurements (returns how many). */
+ * (lanes_per_pairing, threads_per_block, blocks_per_sm) candidate, keep the
+ * fastest in the context, and report up to max_points measurements. */
 int bls_autotune(bls_ctx* ctx, const bls_batch* sample_device, int repeats, bls_tune_point* points,
                  int max_points, int* n_points);
 

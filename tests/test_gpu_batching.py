@@ -60,7 +60,8 @@ def test_autotune_pick_is_exact(wl):
         d_nhms = torch.from_numpy(wl["nhms"].view(np.int64)).cuda()
         d_ids = torch.from_numpy(ids[wl["pk_index"]]).cuda()
         pts = ctx.autotune(n, d_sigs.data_ptr(), d_nhms.data_ptr(), d_ids.data_ptr(), repeats=2)
-        assert len(pts) >= 4 and all(p[2] > 0 for p in pts)
+        assert len(pts) >= 4 and all(p[3] > 0 for p in pts)
+        assert {p[1] for p in pts if p[0] == 6} == {64, 384}          # both block shapes swept
         res = ctx.verify(wl["sigs"], wl["nhms"], ids[wl["pk_index"]])
         assert (res == wl["expect"]).all()
 

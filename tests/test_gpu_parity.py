@@ -11,10 +11,12 @@ import workload_py as W
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=[6, 8, 4, 1], ids=["fp2lanes6", "lanes8", "lanes4", "thread"])
+@pytest.fixture(scope="module", params=[(6, 384), (6, 64), (8, 0), (4, 0), (1, 0)],
+                ids=["fp2lanes6-wide", "fp2lanes6-five", "lanes8", "lanes4", "thread"])
 def ctx(request):
     G.init()
-    with G.Context(lanes=request.param) as c:
+    lanes, tpb = request.param
+    with G.Context(lanes=lanes, threads_per_block=tpb) as c:
         yield c
 
 

@@ -115,11 +115,13 @@ def _submit_all(srv, pool, pk_ids, reqs, threads=3):
     return tickets
 
 
-def test_ring_mode_equals_alone(pool):
+@pytest.mark.parametrize("shape", [384, 64], ids=["wide", "five"])
+def test_ring_mode_equals_alone(pool, shape):
     """Ring mode: one persistent kernel takes items as they are published; every
     request's results equal verifying it alone, for sizes from 1 upwards and a
-    ring smaller than the stream (admission waits for ring space)."""
-    with G.Context() as ctx:
+    ring smaller than the stream (admission waits for ring space), with both
+    block shapes of the kernel."""
+    with G.Context(threads_per_block=shape) as ctx:
         ids = _ids(ctx, pool)
         pk_ids = ids[pool["pk_index"]]
         reqs = _requests(pool, 80, 300, seed=3) + [np.array([7]), np.array([8, 9])]
@@ -136,10 +138,11 @@ def test_ring_mode_equals_alone(pool):
         assert st["launches"] >= 1
 
 
-def test_ring_mode_idle_relaunch(pool):
+@pytest.mark.parametrize("shape", [384, 64], ids=["wide", "five"])
+def test_ring_mode_idle_relaunch(pool, shape):
     """The ring kernel leaves after 20 ms without work; a later request relaunches it."""
     import time
-    with G.Context() as ctx:
+    with G.Context(threads_per_block=shape) as ctx:
         ids = _ids(ctx, pool)
         pk_ids = ids[pool["pk_index"]]
         with G.Server(ctx, max_batch_items=64, mode=G.SERVE_RING) as srv:
@@ -152,7 +155,37 @@ def test_ring_mode_idle_relaunch(pool):
         assert st["launches"] == 3
 
 
-def test_ring_mode_rejects_compressed():
-    with G.Context() as ctx:
-        with pytest.raises(G.GpuError):
-            G.Server(ctx, compressed=True, mode=G.SERVE_RING)
+@pytest.mark.parametrize("shape", [384, 64], ids=["wide", "five"])
+def test_ring_mode_compressed_with_invalid(shape):
+    """Ring mode with 48-byte signatures (the certifier's shares): the
+    dispatcher decodes each published range on the device before the kernel
+    can claim it.  Requests submitted from several threads, with invalid
+    encodings of every kind among them, give exactly the results of verifying
+    each request alone and the workload's known answers."""
+    cc = WL.config_compressed(600, 40, seed=19, invalid_frac=0.05)
+    with G.Context(threads_per_block=shape) as ctx:
+        ids = ctx.register_pk_affine_batch(cc["pk_affine"])
+        pk_ids = ids[cc["pk_index"]]
+        comp = cc["sigs_compressed"]
+        rng = np.random.default_rng(7)
+        cuts = np.unique(np.concatenate([[0, 1, 2, 600], rng.integers(3, 600, 40)]))
+        reqs = [np.arange(a, b) for a, b in zip(cuts[:-1], cuts[1:])]
+        alone = [ctx.verify(comp[ix].reshape(-1), cc["nhms"][ix], pk_ids[ix], compressed=True) for ix in reqs]
+        with G.Server(ctx, compressed=True, max_batch_items=256, mode=G.SERVE_RING, ring_items=400) as srv:
+            tickets = [None] * len(reqs)
+
+            def submit(k0):
+                for k in range(k0, len(reqs), 3):
+                    ix = reqs[k]
+                    tickets[k] = srv.submit(comp[ix], cc["nhms"][ix], pk_ids[ix])
+
+            th = [threading.Thread(target=submit, args=(k,)) for k in range(3)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            for k, (ticket, _, res) in enumerate(tickets):
+                srv.wait(ticket, timeout_ms=60000)
+                assert (res == alone[k]).all()
+                assert (res == cc["expect"][reqs[k]]).all()
+    assert (cc["expect"] < 0).sum() == 30

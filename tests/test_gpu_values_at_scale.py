@@ -35,11 +35,31 @@ ONE_MONT = np.array([0x760900000002FFFD, 0xEBF4000BC40C0002, 0x5F48985753C758BA,
                      0x77CE585370525745, 0x5C071A97A256EC6D, 0x15F65EC3FA80E493], dtype=np.uint64)
 
 
-@pytest.fixture(scope="module")
-def ctx():
+@pytest.fixture(scope="module", params=[384, 64], ids=["wide", "five"])
+def ctx(request):
     G.init()
-    with G.Context(lanes=6) as c:
+    with G.Context(lanes=6, threads_per_block=request.param) as c:
         yield c
+
+
+@pytest.fixture(scope="module")
+def keyset4096():
+    return WL.config_keyset(4096, 40, seed=2)
+
+
+@pytest.fixture(scope="module")
+def keyset40003():
+    return WL.config_keyset(40003, 40, seed=41)
+
+
+@pytest.fixture(scope="module")
+def compressed65536():
+    return WL.config_compressed(65536, 40, seed=3)
+
+
+@pytest.fixture(scope="module")
+def requests256():
+    return WL.config_requests(256, 2048, 40, seed=4)
 
 
 def _register(ctx, wl):
@@ -67,18 +87,16 @@ def _check_values(ctx, g2_table, wl, ids):
     assert ((gt == one).all(axis=1) == (res == 1)).all()
 
 
-def test_keyset_4096_values_exact(ctx, g2_table):
-    wl = WL.config_keyset(4096, 40, seed=2)
-    _check_values(ctx, g2_table, wl, _register(ctx, wl))
+def test_keyset_4096_values_exact(ctx, g2_table, keyset4096):
+    _check_values(ctx, g2_table, keyset4096, _register(ctx, keyset4096))
 
 
-def test_keyset_multi_wave_values_exact(ctx, g2_table):
-    wl = WL.config_keyset(40003, 40, seed=41)
-    _check_values(ctx, g2_table, wl, _register(ctx, wl))
+def test_keyset_multi_wave_values_exact(ctx, g2_table, keyset40003):
+    _check_values(ctx, g2_table, keyset40003, _register(ctx, keyset40003))
 
 
-def test_compressed_slice_values_exact(ctx, g2_table):
-    full = WL.config_compressed(65536, 40, seed=3)
+def test_compressed_slice_values_exact(ctx, g2_table, compressed65536):
+    full = compressed65536
     n = 8192
     comp = np.ascontiguousarray(full["sigs_compressed"][:n])
     nhms = full["nhms"][:n]
@@ -99,8 +117,8 @@ def test_compressed_slice_values_exact(ctx, g2_table):
 
 
 @pytest.mark.parametrize("mode", [G.MODE_PLAIN, G.MODE_PERSISTENT])
-def test_batching_workload_full_size(ctx, g2_table, mode):
-    wl = WL.config_requests(256, 2048, 40, seed=4)
+def test_batching_workload_full_size(ctx, g2_table, mode, requests256):
+    wl = requests256
     assert len(wl["offsets"]) == 257 and len(wl["expect"]) > 60000
     ids = _register(ctx, wl)
     off = wl["offsets"]
