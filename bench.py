@@ -366,6 +366,7 @@ def run_gpu(args):
                    "d2h_bytes_per_step": int(N_ITEMS * 4)}
 
     chain_timad = ctx.imad_chain_rate() / 1e12
+    lo_rate, hi_rate = ctx.imad_pipe_rates()
     batching = serving = ingest = hashing = rlc = compressed = None
     # the single-GPU sections (ingest, hashing, compressed signatures, random
     # linear combinations, batching, serving) run on one GPU only; under torchrun every rank times
@@ -380,7 +381,8 @@ def run_gpu(args):
         if args.serve_seconds > 0:
             serving = run_serving(G, WL, ctx, args.serve_seconds, slots=args.serve_slots,
                                   max_batch=args.serve_max_batch, mode=args.serve_mode,
-                                  ring_blocks_per_sm=args.serve_ring_blocks)
+                                  ring_blocks_per_sm=args.serve_ring_blocks,
+                                  wide=args.lanes == 6 and args.threads_per_block in (0, 384))
 
     result = None
     if rank == 0:
@@ -406,6 +408,19 @@ def run_gpu(args):
             "frac_of_chain_ceiling": round(achieved_timad / chain_timad, 4),
             "chain_ceiling_basis": "measured: 12 x 12-limb carry-chain products (288 IMAD each) in a loop with the "
                                    "verify kernel's block shape and occupancy (bls_imad_chain_rate)",
+            # The nominal peak counts every IMAD at the full rate, but only the
+            # low-word multiply issues at that rate: the high word (mul.hi /
+            # mul.wide) is measured at half of it.  The reference's CIOS
+            # multiply (and this kernel's products) are half low-word and half
+            # high-word multiplies, so the most the pipe can retire of that mix is
+            # the harmonic mean of the two rates.
+            "imad_lo_rate": round(lo_rate / 1e12, 3),
+            "imad_hi_rate": round(hi_rate / 1e12, 3),
+            "mix_peak": round(2.0 / (1e12 / lo_rate + 1e12 / hi_rate), 3),
+            "frac_of_mix_peak": round(achieved_timad / (2.0 / (1e12 / lo_rate + 1e12 / hi_rate)), 4),
+            "mix_peak_basis": "measured (bls_imad_pipe_rates): independent mad.lo.u32 and mad.hi.u32 with every "
+                              "latency covered; a half-low, half-high multiply mix retires at most at their "
+                              "harmonic mean",
         }
         result = {
             "metric": METRIC, "value": round(value, 1), "unit": "verifies/s", "n_gpus": world,
@@ -652,7 +667,7 @@ def run_rlc(G, WL, ctx, wl4096, pk_ids4096, n=65536, reps=3):
 
 
 def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ring", ring_blocks_per_sm=0,
-                ring_blocks=0):
+                ring_blocks=0, wide=True):
     """Serving workload: seeded Poisson stream of requests (sizes log-uniform in
     [1, 512]) over a pool of 40 resident keys, through the continuous-batching
     server (bls_server_*) under a 4 GiB device-memory cap: `mode` "ring" (one
@@ -733,8 +748,11 @@ def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ri
         "p999_ms": round(float(np.percentile(lat, 99.9)), 3), "max_ms": round(float(lat.max()), 3),
         "launches": int(stats1["launches"] - stats0["launches"]),
         "mem_cap_bytes": 4 << 30, "sizes": "log-uniform [1, 512]", "bit_exact": True,
-        "mode": ("ring: one persistent kernel (%d blocks per SM) claiming items five at a time from a device "
-                 "ring" % (ring_blocks_per_sm or 4) if mode == "ring" else "slots: %d launches of up to %d items in flight" % (slots, max_batch)),
+        "mode": (("ring: one persistent twelve-warp block per SM claiming up to 32 published items at a time "
+                  "from a device ring" if wide else
+                  "ring: one persistent kernel (%d five-item blocks per SM) claiming items five at a time from a "
+                  "device ring" % (ring_blocks_per_sm or 4)) if mode == "ring"
+                 else "slots: %d launches of up to %d items in flight" % (slots, max_batch)),
     }
 
 

@@ -115,6 +115,7 @@ def lib():
         L.bls_g1_decompress_status.argtypes = [P, P, I, P, P]
         L.bls_neg_hash_to_g1.argtypes = [P, P, P, I, P, I, P]
         L.bls_imad_chain_rate.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+        L.bls_imad_pipe_rates.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.bls_verify_batch_rlc.argtypes = [P, ctypes.POINTER(Batch), P, P, ctypes.POINTER(I), P]
         L.bls_verify_messages.argtypes = [P, I, P, P, P, P, I, P, I, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
@@ -398,6 +399,12 @@ class Context:
         v = ctypes.c_double(0.0)
         self._check(self.lib.bls_imad_chain_rate(self.h, ctypes.byref(v)), "bls_imad_chain_rate")
         return v.value
+
+    def imad_pipe_rates(self):
+        """(mul.lo, mul.hi) thread instructions per second on the whole device (bls_imad_pipe_rates)."""
+        lo, hi = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self._check(self.lib.bls_imad_pipe_rates(self.h, ctypes.byref(lo), ctypes.byref(hi)), "bls_imad_pipe_rates")
+        return lo.value, hi.value
 
     def g1_decompress(self, compressed):
         src = np.ascontiguousarray(np.frombuffer(bytes(compressed), dtype=np.uint8))

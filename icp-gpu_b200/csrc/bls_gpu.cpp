@@ -848,6 +848,16 @@ int bls_imad_chain_rate(bls_ctx* ctx, double* imad_per_s) {
     return BLS_OK;
 }
 
+int bls_imad_pipe_rates(bls_ctx* ctx, double* lo_per_s, double* hi_per_s) {
+    if (!ctx || !lo_per_s || !hi_per_s) return fail(BLS_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int rc;
+    if ((rc = ctx->grow(ctx->d_in, (size_t)8 * ctx->sms * 256 * 4))) return rc;
+    CK(bls::measure_imad_rates(ctx->sms, 2000, (uint32_t*)ctx->d_in.p, ctx->stream, lo_per_s, hi_per_s));
+    return BLS_OK;
+}
+
 int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* points, int max_points,
                  int* n_points) {
     if (!ctx || !b || b->n <= 0) return fail(BLS_ERR_INVALID, "bad sample");

@@ -104,6 +104,8 @@ cudaError_t launch_verify_w_serve(const VerifyArgs& a, const uint32_t* in_status
 size_t verify_w_smem_bytes();
 int verify_w_blocks_per_sm();
 cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s, double* imad_per_s);
+cudaError_t measure_imad_rates(int sms, int iters, uint32_t* out, cudaStream_t s, double* lo_per_s,
+                               double* hi_per_s);
 size_t verify_lanes_smem_bytes(int lanes, int shape = 0);
 // blocks of the lane-parallel kernel resident per SM (occupancy calculator)
 int verify_lanes_blocks_per_sm(int lanes, int shape = 0);

@@ -571,6 +571,39 @@ __global__ void __launch_bounds__(kThreads, 6) k_imad_chain(int iters, uint32_t*
     out[t] = x;
 }
 
+// Issue rate of one multiply form, device-wide: every thread keeps eight
+// independent accumulators (no dependence between consecutive multiplies of
+// one chain beyond its own), `mode` 0: mul.lo (mad.lo.u32), 1: mul.hi
+// (mad.hi.u32).  32 warps per SM, enough to cover every latency.
+__global__ void __launch_bounds__(256) k_imad_rate(int mode, int iters, uint32_t* out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t acc[8], a[8], b = t * 0x9e3779b9u + 1u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        acc[k] = k;
+        a[k] = 0x85ebca6bu * (t + k) + 7u;
+    }
+    if (mode == 0) {
+#pragma unroll 1
+        for (int i = 0; i < iters; ++i) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) asm volatile("mad.lo.u32 %0, %1, %2, %0;" : "+r"(acc[k]) : "r"(a[k]), "r"(b));
+            b += 0x1234567u;
+        }
+    } else {
+#pragma unroll 1
+        for (int i = 0; i < iters; ++i) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(acc[k]) : "r"(a[k]), "r"(b));
+            b += 0x1234567u;
+        }
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x ^= acc[k];
+    out[t] = x;
+}
+
 cudaError_t configure() {
     static cudaError_t done =
         cudaFuncSetAttribute(k_verify_fp2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes());
@@ -614,6 +647,34 @@ cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (e == cudaSuccess) *imad_per_s = (double)blocks * kThreads * iters * 288.0 / (ms * 1e-3);
+    return e;
+}
+
+// Thread multiply instructions per second of mul.lo and of mul.hi on the whole
+// device (8 blocks of 256 threads per SM); `out` must hold 8 x sms x 256 words.
+cudaError_t measure_imad_rates(int sms, int iters, uint32_t* out, cudaStream_t s, double* lo_per_s,
+                               double* hi_per_s) {
+    const int blocks = 8 * sms;
+    cudaEvent_t a, b;
+    cudaError_t e;
+    if ((e = cudaEventCreate(&a)) != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&b)) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return e;
+    }
+    for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
+        k_imad_rate<<<blocks, 256, 0, s>>>(mode, iters / 10 + 1, out);   // warm-up
+        cudaEventRecord(a, s);
+        k_imad_rate<<<blocks, 256, 0, s>>>(mode, iters, out);
+        cudaEventRecord(b, s);
+        e = cudaEventSynchronize(b);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) *(mode ? hi_per_s : lo_per_s) = (double)blocks * 256 * iters * 8.0 / (ms * 1e-3);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
     return e;
 }
 

@@ -219,6 +219,12 @@ int bls_autotune(bls_ctx* ctx, const bls_batch* sample_device, int repeats, bls_
  * form: mul.lo / mul.hi chained through the carry flag) with the verify
  * kernel's block shape and occupancy, on the whole device. */
 int bls_imad_chain_rate(bls_ctx* ctx, double* imad_per_s);
+/* Measured issue rates of the two halves of a 32 x 32-bit product on the
+ * whole device, in thread instructions per second: mul.lo (the low word) and
+ * mul.hi (the high word), each from independent multiply-adds with every
+ * latency covered.  Their ratio shows how far a multiprecision multiply, half
+ * of whose multiplies are high words, can go toward the nominal IMAD peak. */
+int bls_imad_pipe_rates(bls_ctx* ctx, double* lo_per_s, double* hi_per_s);
 
 /* ---- serving: continuous batching of arriving requests ----
  * A server owns a dispatcher thread and `slots` launch slots (each a stream
