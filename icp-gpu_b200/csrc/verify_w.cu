@@ -497,16 +497,40 @@ __global__ void __launch_bounds__(kThreads, 1) k_verify_w(VerifyArgs a, const ui
             if ((e & f2::kCondMl) && !a.ml_out) continue;
             if (code == f2::kOpLoadLines) {
                 // role (k, h): pair k / 3, coefficient k % 3, component h; a
-                // skipped pair gets the line (0, 0, 1), which leaves f unchanged
+                // skipped pair gets the line (0, 0, 1), which leaves f unchanged.
+                // When the next op is LSCALE (l2 = c1 P.x, l3 = c0 P.y), the roles
+                // holding c1 and c0 form their component of it here: that
+                // program's every output is one product with a zero bias, so
+                // QP(REDC(c_h * P coordinate)) is bit for bit its result, and the
+                // program's exchange and barriers are saved.
+                const bool fuse = st + 1 < seq_len && (f2::kSeq[norm][st + 1] & 31u) == (uint32_t)f2::P_LSCALE;
                 const int pair = k / 3, c = k % 3;
-                const uint32_t slot = kKSlots + kCOff + 6 * pair + c;
+                const uint32_t C = kKSlots + kCOff + 6 * pair;
+                uint32_t x[12];
                 if ((skip >> pair) & 1u) {
-                    store_fp(s, slot, half, (c == 2 && half == 0) ? fp_one().w : fp_zero().w);
+                    const fp v = (c == 2 && half == 0) ? fp_one() : fp_zero();
+#pragma unroll
+                    for (int i = 0; i < 12; ++i) x[i] = v.w[i];
                 } else {
                     const uint64_t* q = pair ? pk : g2_lines;
-                    copy_fp_from_global(s, slot, half, q + 36 * ((e >> 14) & 127u) + 12 * c + 6 * half);
+                    const uint4* g = reinterpret_cast<const uint4*>(q + 36 * ((e >> 14) & 127u) + 12 * c + 6 * half);
+                    const uint4 a0 = __ldg(g), a1 = __ldg(g + 1), a2 = __ldg(g + 2);
+                    x[0] = a0.x; x[1] = a0.y; x[2] = a0.z; x[3] = a0.w;
+                    x[4] = a1.x; x[5] = a1.y; x[6] = a1.z; x[7] = a1.w;
+                    x[8] = a2.x; x[9] = a2.y; x[10] = a2.z; x[11] = a2.w;
+                }
+                store_fp(s, C + c, half, x);
+                if (fuse && c < 2) {
+                    uint32_t y[12], P[26], red[13], o[12];
+                    load_fp(y, s, C + 3, c == 1 ? 0 : 1);   // P.x for l2, P.y for l3
+                    f2::prod24k(P, x, y);
+                    P[24] = P[25] = 0;
+                    f2::redc26(red, P);
+                    f2::qp_reduce(o, red);
+                    store_fp(s, C + (c == 1 ? 4 : 5), half, o);
                 }
                 __syncthreads();
+                if (fuse) ++st;
             } else if (code == f2::kOpLoadCorr) {
                 // the generator's and the key's Miller correction factors into the c2 slots
                 if (k < 2) {
