@@ -42,8 +42,8 @@ SEED = 2
 METRIC = "BLS12-381 verifies/s, batched vs plain launch, bit-exact; serve p50/p99 ms"
 
 # Multiply instructions per verification in this implementation (the
-# six-lane kernel's generated op sequence, counted by gen_fp2ops.py over the
-# 653 programs of one verification): 20,684 products of 12 x 12 limbs, each by
+# six-lane kernels' generated op sequence, counted by gen_fp2ops.py over the
+# 646 programs of one verification): 20,684 products of 12 x 12 limbs, each by
 # one level of limb Karatsuba (three 6 x 6 products: 216 mul.lo / mul.hi), and
 # 7,284 Montgomery reductions (12 rows x 25) = 6,652,944.
 OWN_PRODUCTS_PER_VERIFY = 20684

@@ -521,10 +521,11 @@ def driver_sequence(normalised=False):
             prog("INV%d" % k, d, a)
 
     def cyc_exp(dst, x):
-        # programs may overwrite their inputs, so the products run in place
-        prog("COPY", dst, x)
+        # t = x (the leading bit), then square-and-multiply; the first square
+        # reads x and writes dst, the rest run in place (programs may overwrite
+        # their inputs)
         for i in range(62, -1, -1):
-            prog("CYCSQR", dst, dst)
+            prog("CYCSQR", dst, dst if i < 62 else x)
             if (X_ABS >> i) & 1:
                 prog("MUL", dst, dst, x)
         prog("CONJ", dst, dst)
@@ -532,11 +533,11 @@ def driver_sequence(normalised=False):
     # final exponentiation of group 0 into group 0: the reference's chain,
     # api.cu:65-78, over six groups
     prog("CONJ", 1, 0); inv(2, 0); prog("MUL", 3, 1, 2); prog("FROB", 0, 3); prog("FROB", 1, 0)
-    prog("MUL", 2, 1, 3); prog("COPY", 0, 2); prog("CYCSQR", 0, 0); prog("CONJ", 0, 0)
+    prog("MUL", 2, 1, 3); prog("CYCSQR", 0, 2); prog("CONJ", 0, 0)
     cyc_exp(1, 2)
     prog("MUL", 3, 0, 1)
     cyc_exp(0, 3)
-    prog("CONJ", 3, 3); prog("MUL", 4, 2, 3); prog("COPY", 3, 1); prog("CYCSQR", 3, 3)
+    prog("CONJ", 3, 3); prog("MUL", 4, 2, 3); prog("CYCSQR", 3, 1)
     cyc_exp(5, 0)
     prog("MUL", 1, 1, 5); prog("FROB", 1, 1); prog("FROB", 1, 1); prog("MUL", 1, 4, 1)
     cyc_exp(4, 5)
