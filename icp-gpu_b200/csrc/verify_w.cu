@@ -275,8 +275,9 @@ __device__ __forceinline__ void finish(uint32_t off, const Sm& s, const Bases& b
     f2::qp_reduce(o, r);
 }
 
-// program `pid` for every item of the block: accumulate, exchange, meet,
-// reduce, meet, write, meet.  `role` = 8 half + k (the descriptor index).
+// program `pid` for every item of the block: accumulate, exchange (the two
+// warps of coefficient k meet), reduce, meet, write, meet.  The descriptor
+// index of the role is 8 half + k.
 __device__ __forceinline__ void run(int pid, const Sm& s, int k, int half, const Bases& bs) {
     const uint32_t off = f2::kOutIndex[pid][8 * half + k];
     const uint32_t mode = off != 0xffffu ? (f2::kDesc[off] & 3u) : 0u;
@@ -285,7 +286,10 @@ __device__ __forceinline__ void run(int pid, const Sm& s, int k, int half, const
     const uint4* theirs = s.xch + (k * 2 + (1 - half)) * 7 * kV + s.v;
     uint32_t own[26];
     if (prod) accumulate(off, s, bs, mine, half, own);
-    __syncthreads();
+    // only warps k and 6 + k exchange partial sums here: a named barrier
+    // (id 1 + k) over those 64 threads instead of the whole block; both warps
+    // reach it on every program, whether or not their role has an output
+    asm volatile("bar.sync %0, 64;" ::"r"(1 + k) : "memory");
     uint32_t o[12];
     if (off != 0xffffu) finish(off, s, bs, half, own, theirs, o);
     __syncthreads();
