@@ -853,8 +853,8 @@ int bls_imad_pipe_rates(bls_ctx* ctx, double* lo_per_s, double* hi_per_s) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     CK(cudaSetDevice(ctx->cfg.device));
     int rc;
-    if ((rc = ctx->grow(ctx->d_in, (size_t)8 * ctx->sms * 256 * 4))) return rc;
-    CK(bls::measure_imad_rates(ctx->sms, 2000, (uint32_t*)ctx->d_in.p, ctx->stream, lo_per_s, hi_per_s));
+    if ((rc = ctx->grow(ctx->d_in, (size_t)16 * ctx->sms * 128 * 4))) return rc;
+    CK(bls::measure_imad_rates(ctx->sms, 4096, (uint32_t*)ctx->d_in.p, ctx->stream, lo_per_s, hi_per_s));
     return BLS_OK;
 }
 

@@ -574,8 +574,9 @@ __global__ void __launch_bounds__(kThreads, 6) k_imad_chain(int iters, uint32_t*
 // Issue rate of one multiply form, device-wide: every thread keeps eight
 // independent accumulators (no dependence between consecutive multiplies of
 // one chain beyond its own), `mode` 0: mul.lo (mad.lo.u32), 1: mul.hi
-// (mad.hi.u32).  32 warps per SM, enough to cover every latency.
-__global__ void __launch_bounds__(256) k_imad_rate(int mode, int iters, uint32_t* out) {
+// (mad.hi.u32); the iteration loop is unrolled four times so its counter and
+// branch cost little issue.  64 warps per SM, enough to cover every latency.
+__global__ void __launch_bounds__(128) k_imad_rate(int mode, int iters, uint32_t* out) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t acc[8], a[8], b = t * 0x9e3779b9u + 1u;
 #pragma unroll
@@ -584,14 +585,14 @@ __global__ void __launch_bounds__(256) k_imad_rate(int mode, int iters, uint32_t
         a[k] = 0x85ebca6bu * (t + k) + 7u;
     }
     if (mode == 0) {
-#pragma unroll 1
+#pragma unroll 4
         for (int i = 0; i < iters; ++i) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) asm volatile("mad.lo.u32 %0, %1, %2, %0;" : "+r"(acc[k]) : "r"(a[k]), "r"(b));
             b += 0x1234567u;
         }
     } else {
-#pragma unroll 1
+#pragma unroll 4
         for (int i = 0; i < iters; ++i) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(acc[k]) : "r"(a[k]), "r"(b));
@@ -651,10 +652,10 @@ cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s
 }
 
 // Thread multiply instructions per second of mul.lo and of mul.hi on the whole
-// device (8 blocks of 256 threads per SM); `out` must hold 8 x sms x 256 words.
+// device (16 blocks of 128 threads per SM); `out` must hold 16 x sms x 128 words.
 cudaError_t measure_imad_rates(int sms, int iters, uint32_t* out, cudaStream_t s, double* lo_per_s,
                                double* hi_per_s) {
-    const int blocks = 8 * sms;
+    const int blocks = 16 * sms;
     cudaEvent_t a, b;
     cudaError_t e;
     if ((e = cudaEventCreate(&a)) != cudaSuccess) return e;
@@ -663,15 +664,15 @@ cudaError_t measure_imad_rates(int sms, int iters, uint32_t* out, cudaStream_t s
         return e;
     }
     for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
-        k_imad_rate<<<blocks, 256, 0, s>>>(mode, iters / 10 + 1, out);   // warm-up
+        k_imad_rate<<<blocks, 128, 0, s>>>(mode, iters / 8 * 4 + 4, out);   // warm-up
         cudaEventRecord(a, s);
-        k_imad_rate<<<blocks, 256, 0, s>>>(mode, iters, out);
+        k_imad_rate<<<blocks, 128, 0, s>>>(mode, iters, out);
         cudaEventRecord(b, s);
         e = cudaEventSynchronize(b);
         float ms = 0.f;
         if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
         if (e == cudaSuccess) e = cudaGetLastError();
-        if (e == cudaSuccess) *(mode ? hi_per_s : lo_per_s) = (double)blocks * 256 * iters * 8.0 / (ms * 1e-3);
+        if (e == cudaSuccess) *(mode ? hi_per_s : lo_per_s) = (double)blocks * 128 * iters * 8.0 / (ms * 1e-3);
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
