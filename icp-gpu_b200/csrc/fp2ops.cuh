@@ -131,10 +131,37 @@ __device__ __forceinline__ void mul6(uint32_t* r, const uint32_t* a, const uint3
 // p[0..23] = a * b by one level of Karatsuba on 6-limb halves: L = a0 b0,
 // H = a1 b1, M = (a0 + a1)(b0 + b1) with the halves' carry bits folded in,
 // p = L + (M - L - H) 2^192 + H 2^384.  Three 6 x 6 products (216 multiply
-// instructions) instead of 288; the sums and corrections are plain adds.
+// instructions) instead of 288, computed row by row in lockstep (mul6x3); the
+// sums and corrections are plain adds.
+// three 6 x 6 products r = a b, s = c d, t = e f, row by row in lockstep: the
+// three rows of one step are independent carry chains
+__device__ __forceinline__ void mul6x3(uint32_t* r, const uint32_t* a, const uint32_t* b, uint32_t* s,
+                                       const uint32_t* c, const uint32_t* d, uint32_t* t, const uint32_t* e,
+                                       const uint32_t* f) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        r[j] = a[j] * b[0];
+        s[j] = c[j] * d[0];
+        t[j] = e[j] * f[0];
+    }
+#pragma unroll
+    for (int i = 7; i < 12; ++i) r[i] = s[i] = t[i] = 0;
+    r[6] = s[6] = t[6] = 0;
+    chain_hi6(r, a, b[0]);
+    chain_hi6(s, c, d[0]);
+    chain_hi6(t, e, f[0]);
+#pragma unroll
+    for (int i = 1; i < 6; ++i) {
+        chain_lo6(r + i, a, b[i]);
+        chain_lo6(s + i, c, d[i]);
+        chain_lo6(t + i, e, f[i]);
+        chain_hi6(r + i, a, b[i]);
+        chain_hi6(s + i, c, d[i]);
+        chain_hi6(t + i, e, f[i]);
+    }
+}
+
 __device__ __forceinline__ void prod24k(uint32_t* p, const uint32_t* a, const uint32_t* b) {
-    mul6(p, a, b);
-    mul6(p + 12, a + 6, b + 6);
     uint32_t sa[6], sb[6], ca, cb;
     asm("add.cc.u32 %0, %7, %13;\n\t"
         "addc.cc.u32 %1, %8, %14;\n\t"
@@ -157,7 +184,7 @@ __device__ __forceinline__ void prod24k(uint32_t* p, const uint32_t* a, const ui
         : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]),
           "r"(b[6]), "r"(b[7]), "r"(b[8]), "r"(b[9]), "r"(b[10]), "r"(b[11]));
     uint32_t m[13];
-    mul6(m, sa, sb);
+    mul6x3(p, a, b, p + 12, a + 6, b + 6, m, sa, sb);
     // + ca sb 2^192 + cb sa 2^192 + ca cb 2^384 (m stays below 2^386)
     const uint32_t ma = 0u - ca, mb = 0u - cb;
     asm("add.cc.u32 %0, %0, %7;\n\t"
