@@ -367,7 +367,7 @@ def run_gpu(args):
 
     chain_timad = ctx.imad_chain_rate() / 1e12
     lo_rate, hi_rate = ctx.imad_pipe_rates()
-    batching = serving = ingest = hashing = rlc = compressed = None
+    batching = serving = serving_compressed = ingest = hashing = rlc = compressed = None
     # the single-GPU sections (ingest, hashing, compressed signatures, random
     # linear combinations, batching, serving) run on one GPU only; under torchrun every rank times
     # the headline step alone
@@ -383,6 +383,12 @@ def run_gpu(args):
                                   max_batch=args.serve_max_batch, mode=args.serve_mode,
                                   ring_blocks_per_sm=args.serve_ring_blocks,
                                   wide=args.lanes == 6 and args.threads_per_block in (0, 384))
+        if args.serve_compressed_seconds > 0:
+            serving_compressed = run_serving(G, WL, ctx, args.serve_compressed_seconds, slots=args.serve_slots,
+                                             max_batch=args.serve_max_batch, mode=args.serve_mode,
+                                             ring_blocks_per_sm=args.serve_ring_blocks,
+                                             wide=args.lanes == 6 and args.threads_per_block in (0, 384),
+                                             compressed=True)
 
     result = None
     if rank == 0:
@@ -455,6 +461,8 @@ def run_gpu(args):
             result["batching"] = batching
         if serving:
             result["serving"] = serving
+        if serving_compressed:
+            result["serving_compressed"] = serving_compressed
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(wl, generator_table(WL))
     ctx.close()
@@ -667,33 +675,36 @@ def run_rlc(G, WL, ctx, wl4096, pk_ids4096, n=65536, reps=3):
 
 
 def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ring", ring_blocks_per_sm=0,
-                ring_blocks=0, wide=True):
+                ring_blocks=0, wide=True, compressed=False):
     """Serving workload: seeded Poisson stream of requests (sizes log-uniform in
     [1, 512]) over a pool of 40 resident keys, through the continuous-batching
     server (bls_server_*) under a 4 GiB device-memory cap: `mode` "ring" (one
     persistent kernel claiming items from a device ring as they are published)
-    or "slots" (`slots` launches of up to `max_batch` items in flight).  The
-    arrival rate is `load` x the server's measured saturated throughput;
-    latency is submit to completion on the library's steady clock."""
+    or "slots" (`slots` launches of up to `max_batch` items in flight);
+    `compressed`: the signatures arrive as 48-byte encodings and are decoded on
+    the device.  The arrival rate is `load` x the server's measured saturated
+    throughput; latency is submit to completion on the library's steady clock."""
     import threading
     pool = WL.config_pool(8192, N_KEYS, seed=5)
-    ids = np.array([ctx.register_pk_affine(q) for q in pool["pk_affine"]], dtype=np.int32)
+    ids = ctx.register_pk_affine_batch(pool["pk_affine"])
     pk_ids = ids[pool["pk_index"]]
     npool = len(pool["expect"])
+    sig_src = WL.g1_compress(pool["sigs"]) if compressed else pool["sigs"]
 
     def materialise(starts, sizes):
         out = []
         for a, s in zip(starts, sizes):
             ix = (int(a) + np.arange(int(s))) % npool
-            out.append((ix, np.ascontiguousarray(pool["sigs"][ix]), np.ascontiguousarray(pool["nhms"][ix]),
+            out.append((ix, np.ascontiguousarray(sig_src[ix]), np.ascontiguousarray(pool["nhms"][ix]),
                         np.ascontiguousarray(pk_ids[ix])))
         return out
 
     if mode == "ring":
-        server = G.Server(ctx, max_batch_items=512, mem_cap_bytes=4 << 30, mode=G.SERVE_RING,
-                          ring_blocks_per_sm=ring_blocks_per_sm, ring_blocks=ring_blocks)
+        server = G.Server(ctx, compressed=compressed, max_batch_items=512, mem_cap_bytes=4 << 30,
+                          mode=G.SERVE_RING, ring_blocks_per_sm=ring_blocks_per_sm, ring_blocks=ring_blocks)
     else:
-        server = G.Server(ctx, slots=slots, max_batch_items=max_batch, mem_cap_bytes=4 << 30)
+        server = G.Server(ctx, compressed=compressed, slots=slots, max_batch_items=max_batch,
+                          mem_cap_bytes=4 << 30)
     with server as srv:
         # saturated throughput: a backlog of requests submitted at once
         _, sizes, starts = WL.poisson_stream(1.0, 4000.0, max_size=512, pool_size=npool, seed=7)
@@ -748,6 +759,8 @@ def run_serving(G, WL, ctx, seconds, load=0.8, slots=3, max_batch=8192, mode="ri
         "p999_ms": round(float(np.percentile(lat, 99.9)), 3), "max_ms": round(float(lat.max()), 3),
         "launches": int(stats1["launches"] - stats0["launches"]),
         "mem_cap_bytes": 4 << 30, "sizes": "log-uniform [1, 512]", "bit_exact": True,
+        "signatures": "48-byte compressed, decoded on the device before publication" if compressed
+                      else "affine (96 bytes)",
         "mode": (("ring: one persistent twelve-warp block per SM claiming up to 32 published items at a time "
                   "from a device ring" if wide else
                   "ring: one persistent kernel (%d five-item blocks per SM) claiming items five at a time from a "
@@ -773,6 +786,8 @@ def main():
     ap.add_argument("--compressed-items", type=int, default=65536,
                     help="compressed workload: 48-byte signatures, 2%% invalid encodings (0 = skip)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the serving stream (0 = skip)")
+    ap.add_argument("--serve-compressed-seconds", type=float, default=10.0,
+                    help="length of a second serving stream with 48-byte signatures (0 = skip)")
     ap.add_argument("--serve-mode", choices=["ring", "slots"], default="ring", help="serving: server mode")
     ap.add_argument("--serve-ring-blocks", type=int, default=4,
                     help="serving, ring mode: resident verify blocks per SM")
