@@ -384,11 +384,9 @@ __device__ __forceinline__ void redc26(uint32_t* r, const uint32_t* acc) {
           "r"(t[9]), "r"(t[10]), "r"(t[11]));
 }
 
-// v (13 limbs, below 2^388) -> v - QP[v >> 381], below 2^381 + p (12 limbs)
-__device__ __forceinline__ void qp_reduce(uint32_t* out, const uint32_t* v) {
-    const uint32_t h = (v[12] << 3) | (v[11] >> 29);
-    const uint4* q = reinterpret_cast<const uint4*>(kQP2[h & 127]);
-    const uint4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+// out = v - q (12 limbs; q = QP[v >> 381] in four 16-byte units)
+__device__ __forceinline__ void qp_subtract(uint32_t* out, const uint32_t* v, const uint4& q0, const uint4& q1,
+                                            const uint4& q2, const uint4& q3) {
     uint32_t top;
     asm("sub.cc.u32 %0, %13, %26;\n\t"
         "subc.cc.u32 %1, %14, %27;\n\t"
@@ -409,6 +407,20 @@ __device__ __forceinline__ void qp_reduce(uint32_t* out, const uint32_t* v) {
           "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(q0.x), "r"(q0.y), "r"(q0.z), "r"(q0.w), "r"(q1.x),
           "r"(q1.y), "r"(q1.z), "r"(q1.w), "r"(q2.x), "r"(q2.y), "r"(q2.z), "r"(q2.w), "r"(q3.x));
     (void)top;  // zero: v - QP[h] < 2^384
+}
+
+// v (13 limbs, below 2^388) -> v - QP[v >> 381], below 2^381 + p (12 limbs)
+__device__ __forceinline__ void qp_reduce(uint32_t* out, const uint32_t* v) {
+    const uint32_t h = (v[12] << 3) | (v[11] >> 29);
+    const uint4* q = reinterpret_cast<const uint4*>(kQP2[h & 127]);
+    qp_subtract(out, v, __ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3));
+}
+
+// the same with the QP table copied into shared memory, unit j of entry e at
+// tab[128 j + e] (lanes reading different entries then spread over the banks)
+__device__ __forceinline__ void qp_reduce_tab(uint32_t* out, const uint32_t* v, const uint4* tab) {
+    const uint32_t h = ((v[12] << 3) | (v[11] >> 29)) & 127u;
+    qp_subtract(out, v, tab[h], tab[128 + h], tab[256 + h], tab[384 + h]);
 }
 
 // t[0..12] += c x (x: 12 limbs, |c| < 2^31), modulo 2^416: y = |c| x by

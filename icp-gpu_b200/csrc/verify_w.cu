@@ -41,8 +41,9 @@ constexpr int kXchU4 = 6 * 2 * 7 * kV;           // exchange: 26 words (7 units)
 constexpr int kKpCount = f2::kMaxBias + 1;       // k p, 16 words each
 constexpr int kInfoWords = 4 * kV;               // per item: key index, flags, status, result flags
 constexpr int kFlagBytes = 16 * kV;              // per item and role: "not the expected value" bytes
-constexpr size_t kSmemBytes =
-    (size_t)(kSlotU4 + kKU4 + kXchU4) * 16 + (size_t)kKpCount * 64 + (size_t)kInfoWords * 4 + kFlagBytes + 16;
+constexpr int kQpU4 = 128 * 4;                   // the QP table (128 entries of 16 words)
+constexpr size_t kSmemBytes = (size_t)(kSlotU4 + kKU4 + kXchU4 + kQpU4) * 16 + (size_t)kKpCount * 64 +
+                              (size_t)kInfoWords * 4 + kFlagBytes + 16;
 static_assert(kKSlots + kItemSlots <= 256, "slot indices must fit a byte");
 static_assert(kKpCount <= kThreads, "one thread per table entry at start-up");
 static_assert(kSmemBytes <= 227 * 1024, "one block per SM");
@@ -51,6 +52,7 @@ struct Sm {
     uint4* slots;      // item slots
     uint4* kslots;     // constant slots
     uint4* xch;        // exchange
+    uint4* qp;         // QP table (qp_reduce_tab)
     uint32_t* kp;      // k p table
     uint32_t* info;    // per item: [0] key index, [1] skip bits, [2] status, [3] spare
     uint8_t* flags;    // per item, 16 bytes: role r's "not expected" byte at r
@@ -259,11 +261,11 @@ __device__ __forceinline__ void finish(uint32_t off, const Sm& s, const Bases& b
         uint32_t red[13];
         f2::redc26(red, own);
         if (mode == f2::kModeSimple) {
-            f2::qp_reduce(o, red);
+            f2::qp_reduce_tab(o, red, s.qp);
             return;
         }
         uint32_t q[12];
-        f2::qp_reduce(q, red);
+        f2::qp_reduce_tab(q, red, s.qp);
         load_kp(r, s, bias_lin);
         f2::madd13(r, q, cc);
         for (uint32_t j = 0; j < nl; ++j) {
@@ -272,7 +274,7 @@ __device__ __forceinline__ void finish(uint32_t off, const Sm& s, const Bases& b
             f2::madd13(r, z, sext4(lin[j]));
         }
     }
-    f2::qp_reduce(o, r);
+    f2::qp_reduce_tab(o, r, s.qp);
 }
 
 // program `pid` for every item of the block: accumulate, exchange (the two
@@ -399,7 +401,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_verify_w(VerifyArgs a, const ui
     s.slots = smem4;
     s.kslots = smem4 + kSlotU4;
     s.xch = s.kslots + kKU4;
-    s.kp = reinterpret_cast<uint32_t*>(s.xch + kXchU4);
+    s.qp = s.xch + kXchU4;
+    s.kp = reinterpret_cast<uint32_t*>(s.qp + kQpU4);
     s.info = s.kp + 16 * kKpCount;
     s.flags = reinterpret_cast<uint8_t*>(s.info + kInfoWords);
     s.bcast = reinterpret_cast<uint32_t*>(s.flags + kFlagBytes);
@@ -416,6 +419,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_verify_w(VerifyArgs a, const ui
         f2::set_kp(t, threadIdx.x);
 #pragma unroll
         for (int i = 0; i < 13; ++i) s.kp[16 * threadIdx.x + i] = t[i];
+    }
+    {
+        // unit j of entry e at 128 j + e (qp_reduce_tab)
+        uint32_t* qw = reinterpret_cast<uint32_t*>(s.qp);
+        for (int i = threadIdx.x; i < 128 * 16; i += blockDim.x) {
+            const int e = i / 16, w = i % 16;
+            qw[4 * (128 * (w / 4) + e) + w % 4] = f2::kQP2[e][w];
+        }
     }
     // the flag bytes no role writes (6, 7, 14, 15 of each item) stay zero
     for (int i = threadIdx.x; i < kFlagBytes / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(s.flags)[i] = 0;
@@ -530,7 +541,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_verify_w(VerifyArgs a, const ui
                     f2::prod24k(P, x, y);
                     P[24] = P[25] = 0;
                     f2::redc26(red, P);
-                    f2::qp_reduce(o, red);
+                    f2::qp_reduce_tab(o, red, s.qp);
                     store_fp(s, C + (c == 1 ? 4 : 5), half, o);
                 }
                 __syncthreads();
