@@ -1,7 +1,8 @@
 // Fp inverse by the binary extended Euclidean algorithm, shared by the verify
 // kernels (the final exponentiation's one inversion) and the hash to G1 (the
 // affine result): a few hundred shift-and-subtract passes on 12-limb values
-// instead of the ~570 Montgomery multiplications of a Fermat power.  The
+// instead of the ~570 Montgomery multiplications of a Fermat power; and its
+// warp-wide form, the inverses of a whole warp's values for one Euclid.  The
 // caller passes R^3 mod p (12 limbs, from its generated constants).
 #pragma once
 #include "fp.cuh"
@@ -130,6 +131,64 @@ static __device__ __noinline__ fp fp_inverse_mont(fp x, const uint32_t* kR3) {
 #pragma unroll
     for (int i = 0; i < 12; ++i) r3.w[i] = kR3[i];
     return fp_mul(r, r3);                              // r R^3 / R: Montgomery form of a^-1
+}
+
+
+__device__ __forceinline__ fp shfl_fp(const fp& v, int src) {
+    fp r;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) r.w[i] = __shfl_sync(0xffffffffu, v.w[i], src);
+    return r;
+}
+__device__ __forceinline__ fp shfl_up_fp(const fp& v, int d) {
+    fp r;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) r.w[i] = __shfl_up_sync(0xffffffffu, v.w[i], d);
+    return r;
+}
+__device__ __forceinline__ fp shfl_down_fp(const fp& v, int d) {
+    fp r;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) r.w[i] = __shfl_down_sync(0xffffffffu, v.w[i], d);
+    return r;
+}
+
+// The Fp inverses of the 32 lanes' values by Montgomery's simultaneous-
+// inversion trick over the warp: prefix and suffix products by shuffles (five
+// multiplications each), one inverse of the whole product, which every lane
+// computes from the same value so the binary Euclid's data-dependent branches
+// never split the warp, and two multiplications per lane.  Each lane's own
+// binary Euclid on its own value would diverge and serialise the warp's 32
+// paths.  Every lane of the warp must call it together (full-mask shuffles).
+// z: any value below 2^381 + p; 0 gives 0, as fp_inverse_mont does (a zero
+// stands in as one in the products); kR3: R^3 mod p.
+static __device__ __noinline__ fp fp_inverse_warp(fp z, const uint32_t* kR3) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {          // canonical: fp_mul wants inputs below p
+        uint32_t d[12];
+        const uint32_t br = sub_p(d, z.w);
+#pragma unroll
+        for (int i = 0; i < 12; ++i) z.w[i] = br ? z.w[i] : d[i];
+    }
+    const bool zero = fp_is_zero(z);
+    const fp x = zero ? fp_one() : z;
+    fp pre = x, suf = x;                    // inclusive prefix and suffix products
+    for (int d = 1; d < 32; d <<= 1) {
+        const fp y = shfl_up_fp(pre, d);
+        if (lane >= d) pre = fp_mul_ool(y, pre);
+    }
+    for (int d = 1; d < 32; d <<= 1) {
+        const fp y = shfl_down_fp(suf, d);
+        if (lane + d < 32) suf = fp_mul_ool(suf, y);
+    }
+    const fp total = shfl_fp(pre, 31);
+    fp before = shfl_up_fp(pre, 1), after = shfl_down_fp(suf, 1);
+    if (lane == 0) before = fp_one();
+    if (lane == 31) after = fp_one();
+    const fp t = fp_inverse_mont(total, kR3);
+    const fp r = fp_mul_ool(fp_mul_ool(t, before), after);
+    return zero ? fp_zero() : r;
 }
 
 }  // namespace bls

@@ -199,31 +199,30 @@ static __device__ __noinline__ g1j iso_map(const fp& N, const fp& D, const fp& y
             fp_mul(xden, yden)};
 }
 
-// affine (x, y) of a Jacobian point; false for the identity
-__device__ __forceinline__ bool to_affine(const g1j& p, fp& x, fp& y) {
-    if (fp_is_zero(p.Z)) return false;
-    const fp zi = fp_inverse_mont(p.Z, kR3), zi2 = fp_sqr(zi);
-    x = fp_mul(p.X, zi2);
-    y = fp_mul(p.Y, fp_mul(zi2, zi));
-    return true;
-}
-
-// -H(msg) from the two mapped points, as affine Montgomery (x, y); the
-// identity as x = 0, y = R mod p.  Q = P0 + P1 stays Jacobian through the
-// cofactor clearing [h_eff] Q; one inversion at the end.
-static __device__ __noinline__ void neg_clear(const g1j& p0, const g1j& p1, fp& ox, fp& oy) {
+// [h_eff] (P0 + P1) in Jacobian coordinates: Q = P0 + P1 stays Jacobian
+// through the cofactor clearing.
+static __device__ __noinline__ g1j clear_sum(const g1j& p0, const g1j& p1) {
     const g1j q = g1j_add(p0, p1);
     g1j r = q;
     for (int i = 62; i >= 0; --i) {
         r = g1j_dbl(r);
         if ((kHEff >> i) & 1) r = g1j_add(r, q);
     }
-    fp rx, ry;
-    ox = fp_zero();
-    oy = fp_one();
-    if (!to_affine(r, rx, ry)) return;
-    ox = rx;
-    oy = fp_neg(ry);
+    return r;
+}
+
+// -H(msg) as affine Montgomery (x, y) from r = [h_eff](P0 + P1) and zi =
+// 1 / r.Z (the caller's inversion); the identity (r.Z = 0) as x = 0,
+// y = R mod p.
+__device__ __forceinline__ void neg_affine(const g1j& r, const fp& zi, fp& ox, fp& oy) {
+    if (fp_is_zero(r.Z)) {
+        ox = fp_zero();
+        oy = fp_one();
+        return;
+    }
+    const fp zi2 = fp_sqr(zi);
+    ox = fp_mul(r.X, zi2);
+    oy = fp_neg(fp_mul(r.Y, fp_mul(zi2, zi)));
 }
 
 }  // namespace h2c

@@ -40,19 +40,30 @@ __global__ void __launch_bounds__(kHashThreads) k_neg_hash_to_g1(const uint8_t* 
         }
     }
     __syncthreads();
-    if (!live || which) return;
-    const uint4* d = xch[threadIdx.x >> 1];
-    g1j p1;
-    fp* c[3] = {&p1.X, &p1.Y, &p1.Z};
+    // the even thread of a live message adds the points and clears the
+    // cofactor; then every thread of the warp takes part in one simultaneous
+    // inversion of the results' Z (the others contribute a one), so the
+    // warp's 16 inverses cost one binary Euclid that does not diverge
+    const bool owner = live && !which;
+    g1j r;
+    r.Z = fp_one();
+    if (owner) {
+        const uint4* d = xch[threadIdx.x >> 1];
+        g1j p1;
+        fp* c[3] = {&p1.X, &p1.Y, &p1.Z};
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const uint4 q = d[3 * k + j];
-            c[k]->w[4 * j] = q.x; c[k]->w[4 * j + 1] = q.y; c[k]->w[4 * j + 2] = q.z; c[k]->w[4 * j + 3] = q.w;
-        }
+            for (int j = 0; j < 3; ++j) {
+                const uint4 q = d[3 * k + j];
+                c[k]->w[4 * j] = q.x; c[k]->w[4 * j + 1] = q.y; c[k]->w[4 * j + 2] = q.z; c[k]->w[4 * j + 3] = q.w;
+            }
+        r = h2c::clear_sum(pt, p1);
+    }
+    const fp zi = fp_inverse_warp(owner ? r.Z : fp_one(), h2c::kR3);
+    if (!owner) return;
     fp ox, oy;
-    h2c::neg_clear(pt, p1, ox, oy);
+    h2c::neg_affine(r, zi, ox, oy);
     fp_store_u64(out + 12 * (size_t)i, ox);
     fp_store_u64(out + 12 * (size_t)i + 6, oy);
 }

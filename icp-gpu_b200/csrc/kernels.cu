@@ -88,7 +88,9 @@ __global__ void __launch_bounds__(64) k_g2_prepare(const uint64_t* q, int n, uin
 }
 
 // One line table per block, one row per thread: every row (c0, c1, c2)
-// becomes (c0 / c2, c1 / c2, 1), each thread inverting its own c2, and the
+// becomes (c0 / c2, c1 / c2, 1), 1 / c2 = conj(c2) / |c2| with the norms of a
+// warp's 32 rows inverted together (fp_inverse_warp: one binary Euclid per
+// warp, not one divergent Euclid per row), and the
 // Miller correction factor prod_i c2_i^(2^s_i) is formed in parallel: s_i is
 // the number of squarings that follow line i in the Miller loop's order of
 // lines and squarings (api.cu:30-52), each thread squares its c2 s_i times,
@@ -132,8 +134,13 @@ __global__ void __launch_bounds__(kNormThreads) k_lines_normalize(const uint64_t
         }
         return;
     }
+    // every thread of the block takes part in its warp's inversion (rows past
+    // the table contribute a one)
+    const fp c2_norm = fp_add(fp_sqr(c2.c0), fp_sqr(c2.c1));
+    const fp r3 = fp_mul(fp_rr(), fp_rr());                        // R^3 mod p
+    const fp ninv = fp_inverse_warp(c2_norm, r3.w);
     if (i < kNormRows) {
-        const fp2 inv = fp2_inv(c2);
+        const fp2 inv = {fp_mul(c2.c0, ninv), fp_neg(fp_mul(c2.c1, ninv))};
         const fp2 c0 = {fp_load_u64(in + 36 * i), fp_load_u64(in + 36 * i + 6)};
         const fp2 c1 = {fp_load_u64(in + 36 * i + 12), fp_load_u64(in + 36 * i + 18)};
         store_fp2(out + 36 * i, fp2_mul(c0, inv));

@@ -108,8 +108,13 @@ struct Ring {
 };
 constexpr int32_t kSentinel = 0x7fffffff;
 // SMs left free of the twelve-warp ring kernel for the decoder of compressed
-// signatures (a block of the decoder does not fit beside a resident block)
-constexpr int kDecodeSms = 4;
+// signatures (a block of the decoder does not fit beside a resident block).
+// The decoder takes one thread per point through a chain of about 1,600
+// multiplications (the square root and the subgroup check), some 4 ms, with
+// three blocks of 128 threads per SM: about 96 k points/s per SM, so 12 SMs
+// keep it ahead of the verify rate of the other 136 at 80% load (4 SMs left
+// it saturated and queueing).
+constexpr int kDecodeSms = 12;
 
 struct bls_server {
     bls_ctx* ctx = nullptr;

@@ -133,62 +133,6 @@ __device__ __forceinline__ void xch_load(uint32_t* p, const uint4* row) {
     p[25] = u.y;
 }
 
-__device__ __forceinline__ fp shfl_fp(const fp& v, int src) {
-    fp r;
-#pragma unroll
-    for (int i = 0; i < 12; ++i) r.w[i] = __shfl_sync(0xffffffffu, v.w[i], src);
-    return r;
-}
-__device__ __forceinline__ fp shfl_up_fp(const fp& v, int d) {
-    fp r;
-#pragma unroll
-    for (int i = 0; i < 12; ++i) r.w[i] = __shfl_up_sync(0xffffffffu, v.w[i], d);
-    return r;
-}
-__device__ __forceinline__ fp shfl_down_fp(const fp& v, int d) {
-    fp r;
-#pragma unroll
-    for (int i = 0; i < 12; ++i) r.w[i] = __shfl_down_sync(0xffffffffu, v.w[i], d);
-    return r;
-}
-
-// The Fp inverses of the 32 lanes' values (one per item) by Montgomery's
-// simultaneous-inversion trick over the warp: prefix and suffix products by
-// shuffles (five multiplications each), one inverse of the whole product,
-// which every lane computes from the same value so the binary Euclid's
-// data-dependent branches never split the warp, and two multiplications per
-// lane.  Each lane's own binary Euclid would diverge across the 32 items and
-// serialise their paths.  z: any value below 2^381 + p; 0 gives 0, as
-// fp_inverse_mont does (a zero stands in as one in the products).
-__device__ __noinline__ fp warp_inverse(fp z) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {          // canonical: fp_mul wants inputs below p
-        uint32_t d[12];
-        const uint32_t br = sub_p(d, z.w);
-#pragma unroll
-        for (int i = 0; i < 12; ++i) z.w[i] = br ? z.w[i] : d[i];
-    }
-    const bool zero = fp_is_zero(z);
-    const fp x = zero ? fp_one() : z;
-    fp pre = x, suf = x;                    // inclusive prefix and suffix products
-    for (int d = 1; d < 32; d <<= 1) {
-        const fp y = shfl_up_fp(pre, d);
-        if (lane >= d) pre = fp_mul_ool(y, pre);
-    }
-    for (int d = 1; d < 32; d <<= 1) {
-        const fp y = shfl_down_fp(suf, d);
-        if (lane + d < 32) suf = fp_mul_ool(suf, y);
-    }
-    const fp total = shfl_fp(pre, 31);
-    fp before = shfl_up_fp(pre, 1), after = shfl_down_fp(suf, 1);
-    if (lane == 0) before = fp_one();
-    if (lane == 31) after = fp_one();
-    const fp t = fp_inverse_mont(total, f2::kR3);
-    const fp r = fp_mul_ool(fp_mul_ool(t, before), after);
-    return zero ? fp_zero() : r;
-}
-
 // Phase 1 of an output (product modes): this half's products into both
 // accumulators; the partner's component (accX) goes to the exchange row.
 __device__ __forceinline__ void accumulate(uint32_t off, const Sm& s, const Bases& bs, uint4* xch_out, int half,
@@ -293,7 +237,7 @@ __device__ __forceinline__ void finish(uint32_t off, const Sm& s, const Bases& b
         if (half == 0) {
             fp z;
             load_fp(z.w, s, slot_addr(bs, lin[0] >> 8), 0);
-            fp r = warp_inverse(z);
+            fp r = fp_inverse_warp(z, f2::kR3);
 #pragma unroll
             for (int i = 0; i < 12; ++i) o[i] = r.w[i];
         } else {
