@@ -40,6 +40,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <utility>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -96,7 +97,18 @@ struct Ring {
     int32_t *d_ids = nullptr, *d_res = nullptr;
     uint32_t* d_ctl = nullptr;             // device: [0] published, [1] stop, [2] claimed
     cudaStream_t copy = nullptr, kern = nullptr;
+    cudaStream_t poll = nullptr;           // result reads, apart from the copy stream's decodes
     cudaEvent_t done = nullptr;
+    // Publications do not wait: round r copies its count from its own pinned
+    // word (h_pubv[r % kPubSlots]) and records pub_ev[r % kPubSlots] after the
+    // copy; `confirmed` is the count of the newest publication known to have
+    // landed, and only [tail, confirmed) is ever read back (results beyond it
+    // may still be a slot's earlier contents on the device).
+    static constexpr int kPubSlots = 64;
+    uint32_t* h_pubv = nullptr;
+    cudaEvent_t pub_ev[kPubSlots] = {};
+    std::deque<std::pair<int, uint32_t>> pub_pending;
+    uint32_t confirmed = 0, pub_round = 0;
     bool launched = false;
     uint32_t pub = 0, tail = 0;            // items published / released (monotonic)
     struct Flight {
@@ -261,14 +273,24 @@ struct bls_server {
     // that submitters and waiters never queue behind a copy or a sync.
     int ring_step(std::unique_lock<std::mutex>& lk, bool& progressed) {
         lk.unlock();
-        const uint32_t inflight = ring.pub - ring.tail;
+        while (!ring.pub_pending.empty()) {   // publications that have landed
+            const cudaError_t q = cudaEventQuery(ring.pub_ev[ring.pub_pending.front().first]);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) {
+                lk.lock();
+                return BLS_ERR_CUDA;
+            }
+            ring.confirmed = ring.pub_pending.front().second;
+            ring.pub_pending.pop_front();
+        }
+        const uint32_t inflight = ring.confirmed - ring.tail;
         if (inflight) {
             const uint32_t s0 = ring.tail % ring.cap, first = std::min(inflight, ring.cap - s0);
             if (cudaMemcpyAsync(ring.h_res + s0, ring.d_res + s0, 4 * (size_t)first, cudaMemcpyDeviceToHost,
-                                ring.copy) ||
+                                ring.poll) ||
                 (first < inflight && cudaMemcpyAsync(ring.h_res, ring.d_res, 4 * (size_t)(inflight - first),
-                                                     cudaMemcpyDeviceToHost, ring.copy)) ||
-                cudaStreamSynchronize(ring.copy)) {
+                                                     cudaMemcpyDeviceToHost, ring.poll)) ||
+                cudaStreamSynchronize(ring.poll)) {
                 lk.lock();
                 return BLS_ERR_CUDA;
             }
@@ -351,13 +373,24 @@ struct bls_server {
                 lk.lock();
                 return rc;
             }
-            // the count goes up only after the items' copies (same stream)
-            ring.h_ctl[0] = ring.pub;
-            if (cudaMemcpyAsync(ring.d_ctl, ring.h_ctl, 4, cudaMemcpyHostToDevice, ring.copy) ||
-                cudaStreamSynchronize(ring.copy)) {
+            // the count goes up only after the items' copies (and decode) on the
+            // same stream; nothing waits for it here
+            if ((int)ring.pub_pending.size() == Ring::kPubSlots) {   // every word in use: wait for the oldest
+                if (cudaEventSynchronize(ring.pub_ev[ring.pub_pending.front().first]) != cudaSuccess) {
+                    lk.lock();
+                    return BLS_ERR_CUDA;
+                }
+                ring.confirmed = ring.pub_pending.front().second;
+                ring.pub_pending.pop_front();
+            }
+            const int slot = (int)(ring.pub_round++ % Ring::kPubSlots);
+            ring.h_pubv[slot] = ring.pub;
+            if (cudaMemcpyAsync(ring.d_ctl, ring.h_pubv + slot, 4, cudaMemcpyHostToDevice, ring.copy) ||
+                cudaEventRecord(ring.pub_ev[slot], ring.copy)) {
                 lk.lock();
                 return BLS_ERR_CUDA;
             }
+            ring.pub_pending.emplace_back(slot, ring.pub);
             progressed = true;
         }
         bool pending = false, relaunched = false;
@@ -502,9 +535,13 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
                              cudaMalloc((void**)&r.d_comp, cap * 48) == cudaSuccess &&
                              cudaMalloc((void**)&r.d_st, cap * 4) == cudaSuccess)) &&
                   cudaStreamCreateWithFlags(&r.copy, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&r.poll, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaHostAlloc((void**)&r.h_pubv, 4 * Ring::kPubSlots, 0) == cudaSuccess &&
                   cudaStreamCreateWithFlags(&r.kern, cudaStreamNonBlocking) == cudaSuccess &&
                   cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming) == cudaSuccess &&
                   cudaDeviceSynchronize() == cudaSuccess;
+        for (int k = 0; ok && k < Ring::kPubSlots; ++k)
+            ok = cudaEventCreateWithFlags(&r.pub_ev[k], cudaEventDisableTiming) == cudaSuccess;
         if (ok) memset(r.h_ctl, 0, 64);
         if (!ok) {
             bls_server_destroy(s);
@@ -560,8 +597,11 @@ void bls_server_destroy(bls_server* s) {
         Ring& r = s->ring;
         s->ring_stop();
         for (void* p : {(void*)r.h_sigs, (void*)r.h_nhms, (void*)r.h_ids, (void*)r.h_res, (void*)r.h_ctl,
-                        (void*)r.h_comp})
+                        (void*)r.h_comp, (void*)r.h_pubv})
             if (p) cudaFreeHost(p);
+        for (cudaEvent_t ev : r.pub_ev)
+            if (ev) cudaEventDestroy(ev);
+        if (r.poll) cudaStreamDestroy(r.poll);
         for (void* p : {(void*)r.d_sigs, (void*)r.d_nhms, (void*)r.d_ids, (void*)r.d_res, (void*)r.d_ctl,
                         (void*)r.d_comp, (void*)r.d_st})
             if (p) cudaFree(p);
