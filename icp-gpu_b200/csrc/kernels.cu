@@ -87,30 +87,45 @@ __global__ void __launch_bounds__(64) k_g2_prepare(const uint64_t* q, int n, uin
     g2_prepare(qx, qy, out + BLS_COEFF_U64 * (size_t)i);
 }
 
-// One line table per block, one row per thread: every row (c0, c1, c2)
-// becomes (c0 / c2, c1 / c2, 1), 1 / c2 = conj(c2) / |c2| with the norms of a
-// warp's 32 rows inverted together (fp_inverse_warp: one binary Euclid per
-// warp, not one divergent Euclid per row).  Thread 0 forms the Miller
-// correction factor prod_i c2_i^(2^(squarings after line i)) by the Miller
-// loop's own order of lines and squarings (api.cu:30-52), Horner-wise: 62
-// squarings and 68 products, from the c2 values the rows left in shared
-// memory.  Every operation returns the canonical representative.  A table
-// with a zero c2 is copied unchanged and flagged.
+// Small key sets: one line table per block, one row per thread, so a table's
+// latency is about one row's work.  Every row (c0, c1, c2) becomes
+// (c0 / c2, c1 / c2, 1), 1 / c2 = conj(c2) / |c2| with the norms of a warp's
+// 32 rows inverted together (fp_inverse_warp: one binary Euclid per warp, not
+// one divergent Euclid per row), and the
+// Miller correction factor prod_i c2_i^(2^s_i) is formed in parallel: s_i is
+// the number of squarings that follow line i in the Miller loop's order of
+// lines and squarings (api.cu:30-52), each thread squares its c2 s_i times,
+// and a product tree in shared memory multiplies the 68 powers.  Every
+// operation returns the canonical representative, so the values do not depend
+// on the order of the products.  A table with a zero c2 is copied unchanged
+// and flagged.
 constexpr int kNormRows = 68;
 constexpr int kNormThreads = 128;
 
-__global__ void __launch_bounds__(kNormThreads) k_lines_normalize(const uint64_t* raw, int n, uint64_t* norm,
+// squarings after line `row` of the Miller loop: lines taken in iteration b
+// (b = 61 .. 0 over the bits of |x| >> 1 below the leading one) are squared
+// b + 1 times; the last line (after the loop) none
+__device__ __forceinline__ int squarings_after(int row) {
+    const uint64_t xabs = 0xd201000000010000ULL;
+    int ci = 0;
+    for (int b = 61; b >= 0; --b) {
+        if (ci++ == row) return b + 1;
+        if (((xabs >> 1) >> b) & 1) {
+            if (ci++ == row) return b + 1;
+        }
+    }
+    return 0;
+}
+
+__global__ void __launch_bounds__(kNormThreads) k_lines_normalize_rows(const uint64_t* raw, int n, uint64_t* norm,
                                                                   uint64_t* corr, uint8_t* bad) {
-    __shared__ uint64_t c2s[kNormRows][12];
+    __shared__ uint64_t pw[kNormRows][12];
     const int t = blockIdx.x, i = threadIdx.x;
     if (t >= n) return;   // the whole block leaves together
     const uint64_t* in = raw + BLS_COEFF_U64 * (size_t)t;
     uint64_t* out = norm + BLS_COEFF_U64 * (size_t)t;
     fp2 c2 = fp2_one();
-    if (i < kNormRows) {
-        c2 = fp2{fp_load_u64(in + 36 * i + 24), fp_load_u64(in + 36 * i + 30)};
-        store_fp2(c2s[i], c2);
-    }
+    if (i < kNormRows) c2 = fp2{fp_load_u64(in + 36 * i + 24), fp_load_u64(in + 36 * i + 30)};
     const bool zero = __syncthreads_or(i < kNormRows && fp2_is_zero(c2));
     if (zero) {
         for (int k = i; k < BLS_COEFF_U64; k += kNormThreads) out[k] = in[k];
@@ -132,27 +147,89 @@ __global__ void __launch_bounds__(kNormThreads) k_lines_normalize(const uint64_t
         store_fp2(out + 36 * i, fp2_mul(c0, inv));
         store_fp2(out + 36 * i + 12, fp2_mul(c1, inv));
         store_fp2(out + 36 * i + 24, fp2_one());
+        fp2 p = c2;
+        for (int k = squarings_after(i); k > 0; --k) p = fp2_sqr(p);
+        store_fp2(pw[i], p);
+    }
+    __syncthreads();
+    for (int stride = 1; stride < kNormRows; stride *= 2) {
+        if (i % (2 * stride) == 0 && i + stride < kNormRows) {
+            const fp2 a = {fp_load_u64(pw[i]), fp_load_u64(pw[i] + 6)};
+            const fp2 b = {fp_load_u64(pw[i + stride]), fp_load_u64(pw[i + stride] + 6)};
+            store_fp2(pw[i], fp2_mul(a, b));
+        }
+        __syncthreads();
     }
     if (i == 0) {
-        auto c2_of = [&](int r) { return fp2{fp_load_u64(c2s[r]), fp_load_u64(c2s[r] + 6)}; };
-        const uint64_t xabs = 0xd201000000010000ULL;
-        fp2 cf = fp2_one();
-        int ci = 0;
-        for (int b = 61; b >= 0; --b) {
-            cf = fp2_mul(cf, c2_of(ci++));
-            if (((xabs >> 1) >> b) & 1) cf = fp2_mul(cf, c2_of(ci++));
-            cf = fp2_sqr(cf);
-        }
-        cf = fp2_mul(cf, c2_of(ci));
-        store_fp2(corr + 12 * (size_t)t, cf);
+        store_fp2(corr + 12 * (size_t)t, fp2{fp_load_u64(pw[0]), fp_load_u64(pw[0] + 6)});
         bad[t] = 0;
     }
 }
 
+// Large key sets: one line table per thread, every row (c0, c1, c2) becomes (c0 / c2, c1 / c2, 1)
+// (inverses by Montgomery's batch trick: one Fp2 inverse per table), and the
+// Miller correction factor prod_i c2_i^(2^(squarings after line i)) follows the
+// Miller loop's order of lines and squarings (api.cu:30-52).  A table with a
+// zero c2 is copied unchanged and flagged.
+__global__ void __launch_bounds__(64) k_lines_normalize_table(const uint64_t* raw, int n, uint64_t* norm, uint64_t* corr,
+                                                      uint8_t* bad) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint64_t* in = raw + BLS_COEFF_U64 * (size_t)t;
+    uint64_t* out = norm + BLS_COEFF_U64 * (size_t)t;
+    constexpr int kRows = 68;
+    auto c2_of = [&](int i) { return fp2{fp_load_u64(in + 36 * i + 24), fp_load_u64(in + 36 * i + 30)}; };
+    // prefix products of c2 in the output's c2 slots
+    fp2 pre = fp2_one();
+    for (int i = 0; i < kRows; ++i) {
+        pre = fp2_mul(pre, c2_of(i));
+        store_fp2(out + 36 * i + 24, pre);
+    }
+    if (fp2_is_zero(pre)) {
+        for (int i = 0; i < BLS_COEFF_U64; ++i) out[i] = in[i];
+        store_fp2(corr + 12 * (size_t)t, fp2_one());
+        bad[t] = 1;
+        return;
+    }
+    fp2 inv = fp2_inv(pre);   // (c2_0 ... c2_67)^-1
+    for (int i = kRows - 1; i >= 0; --i) {
+        fp2 c2 = c2_of(i);
+        fp2 inv_i = i ? fp2_mul(inv, fp2{fp_load_u64(out + 36 * (i - 1) + 24), fp_load_u64(out + 36 * (i - 1) + 30)})
+                      : inv;
+        inv = fp2_mul(inv, c2);
+        fp2 c0 = {fp_load_u64(in + 36 * i), fp_load_u64(in + 36 * i + 6)};
+        fp2 c1 = {fp_load_u64(in + 36 * i + 12), fp_load_u64(in + 36 * i + 18)};
+        store_fp2(out + 36 * i, fp2_mul(c0, inv_i));
+        store_fp2(out + 36 * i + 12, fp2_mul(c1, inv_i));
+    }
+    for (int i = 0; i < kRows; ++i) store_fp2(out + 36 * i + 24, fp2_one());
+    // correction factor
+    const uint64_t xabs = 0xd201000000010000ULL;
+    fp2 cf = fp2_one();
+    int ci = 0;
+    for (int b = 61; b >= 0; --b) {
+        cf = fp2_mul(cf, c2_of(ci++));
+        if (((xabs >> 1) >> b) & 1) cf = fp2_mul(cf, c2_of(ci++));
+        cf = fp2_sqr(cf);
+    }
+    cf = fp2_mul(cf, c2_of(ci));
+    store_fp2(corr + 12 * (size_t)t, cf);
+    bad[t] = 0;
+}
+
+// A key set of at most kRowsMaxTables tables takes the row-parallel form (low
+// latency: one block per table); a larger one the table-per-thread form
+// (least work: the whole set in one wave, where the row form would square each
+// row's c2 separately and take many waves).
+constexpr int kRowsMaxTables = 2048;
+
 cudaError_t launch_lines_normalize(const uint64_t* raw, int n, uint64_t* norm, uint64_t* corr, uint8_t* bad,
                                    cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    k_lines_normalize<<<n, kNormThreads, 0, s>>>(raw, n, norm, corr, bad);
+    if (n <= kRowsMaxTables)
+        k_lines_normalize_rows<<<n, kNormThreads, 0, s>>>(raw, n, norm, corr, bad);
+    else
+        k_lines_normalize_table<<<(n + 63) / 64, 64, 0, s>>>(raw, n, norm, corr, bad);
     return cudaGetLastError();
 }
 

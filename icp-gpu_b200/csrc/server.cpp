@@ -316,13 +316,18 @@ struct bls_server {
             ring.tail += ring.flights.front().span;
             ring.flights.pop_front();
         }
-        // completions out, admissions in: the only part under the mutex
+        // completions out, admissions in: the only part under the mutex.  With
+        // compressed signatures a round's decode takes one point's whole chain
+        // (about 4 ms) whatever its size, and rounds run one after another on
+        // the copy stream, so a new round is admitted only once the previous
+        // one has been published: requests that arrive meanwhile join it.
         std::vector<Pending> admit;
         uint32_t room = ring.cap - (ring.pub - ring.tail);
+        const bool admitting = !(ring.h_comp && !ring.pub_pending.empty());
         lk.lock();
         for (uint64_t tk : finished) done[tk] = t;
         items += finished_items;
-        while (!queue.empty()) {
+        while (admitting && !queue.empty()) {
             const uint32_t span = ((uint32_t)queue.front().n + ring.group - 1) / ring.group * ring.group;
             if (span > room) break;
             room -= span;
