@@ -22,14 +22,9 @@ __device__ __forceinline__ bool u_is_one(const uint32_t* u) {
     return o == 0;
 }
 __device__ __forceinline__ bool geq12(const uint32_t* a, const uint32_t* b) {
-    uint32_t d[12], br = 0;
+    uint32_t br = 0;
 #pragma unroll
-    for (int i = 0; i < 12; ++i) {
-        uint64_t t = (uint64_t)a[i] - b[i] - br;
-        d[i] = (uint32_t)t;
-        br = (uint32_t)(t >> 63);
-    }
-    (void)d;
+    for (int i = 0; i < 12; ++i) br = (uint32_t)(((uint64_t)a[i] - b[i] - br) >> 63);
     return br == 0;
 }
 __device__ __forceinline__ void sub12(uint32_t* a, const uint32_t* b) {

@@ -89,8 +89,12 @@ struct Ring {
     int32_t *h_ids = nullptr, *h_res = nullptr;      // cap
     uint32_t* h_ctl = nullptr;             // pinned: [0] published items, [1] stop
     // compressed signatures: 48-byte encodings in (pinned mirror and device),
-    // decoded into d_sigs with a per-slot status by the decoder on the copy
-    // stream before the range is published
+    // decoded into d_sigs with a per-slot status before the range is
+    // published; up to kDecStreams rounds decode at once, round r on
+    // dec[r % kDecStreams], and each round's publication waits for the one
+    // before it, so the published count only ever covers decoded slots
+    static constexpr int kDecStreams = 4;
+    cudaStream_t dec[kDecStreams] = {};
     uint8_t *h_comp = nullptr, *d_comp = nullptr;
     int32_t* d_st = nullptr;
     uint64_t *d_sigs = nullptr, *d_nhms = nullptr;
@@ -121,12 +125,13 @@ struct Ring {
 constexpr int32_t kSentinel = 0x7fffffff;
 // SMs left free of the twelve-warp ring kernel for the decoder of compressed
 // signatures (a block of the decoder does not fit beside a resident block).
-// The decoder takes one thread per point through a chain of about 1,600
-// multiplications (the square root and the subgroup check), some 4 ms, with
-// three blocks of 128 threads per SM: about 96 k points/s per SM, so 12 SMs
-// keep it ahead of the verify rate of the other 136 at 80% load (4 SMs left
-// it saturated and queueing).
-constexpr int kDecodeSms = 12;
+// The decoder takes one thread per point through a chain of about 1,300
+// multiplication-equivalents (the square root's 376 squarings and 85
+// products, the subgroup check's 127 doublings), a few ms, with three blocks
+// of 128 threads per SM.  The split balances the two rates: a verify costs
+// the ring kernel about 280 k SM-cycles and a decode about 28 k, so 14 of
+// 148 SMs decode (12 left the decoder the bottleneck of a saturated ring).
+constexpr int kDecodeSms = 14;
 
 struct bls_server {
     bls_ctx* ctx = nullptr;
@@ -243,24 +248,23 @@ struct bls_server {
 
     // host mirror range [a, a + n) (ring positions, may wrap) to the device
     template <typename T>
-    int ring_copy_in(T* dst, const T* src, size_t per, uint32_t a, uint32_t n) {
+    int ring_copy_in(T* dst, const T* src, size_t per, uint32_t a, uint32_t n, cudaStream_t st) {
         const uint32_t s0 = a % ring.cap, first = std::min(n, ring.cap - s0);
-        if (cudaMemcpyAsync(dst + per * s0, src + per * s0, sizeof(T) * per * first, cudaMemcpyHostToDevice,
-                            ring.copy))
+        if (cudaMemcpyAsync(dst + per * s0, src + per * s0, sizeof(T) * per * first, cudaMemcpyHostToDevice, st))
             return BLS_ERR_CUDA;
-        if (first < n && cudaMemcpyAsync(dst, src, sizeof(T) * per * (n - first), cudaMemcpyHostToDevice, ring.copy))
+        if (first < n && cudaMemcpyAsync(dst, src, sizeof(T) * per * (n - first), cudaMemcpyHostToDevice, st))
             return BLS_ERR_CUDA;
         return BLS_OK;
     }
 
-    // decode ring range [a, a + n) (may wrap) on the copy stream: the decoded
+    // decode ring range [a, a + n) (may wrap) on stream st: the decoded
     // points into d_sigs, each slot's decode status into d_st
-    int ring_decode(uint32_t a, uint32_t n) {
+    int ring_decode(uint32_t a, uint32_t n, cudaStream_t st) {
         const uint32_t s0 = a % ring.cap, first = std::min(n, ring.cap - s0);
         if (bls::launch_g1_decompress(ring.d_comp + 48 * (size_t)s0, (int)first, ring.d_sigs + 12 * (size_t)s0,
-                                      ring.d_st + s0, ring.copy))
+                                      ring.d_st + s0, st))
             return BLS_ERR_CUDA;
-        if (first < n && bls::launch_g1_decompress(ring.d_comp, (int)(n - first), ring.d_sigs, ring.d_st, ring.copy))
+        if (first < n && bls::launch_g1_decompress(ring.d_comp, (int)(n - first), ring.d_sigs, ring.d_st, st))
             return BLS_ERR_CUDA;
         return BLS_OK;
     }
@@ -318,12 +322,12 @@ struct bls_server {
         }
         // completions out, admissions in: the only part under the mutex.  With
         // compressed signatures a round's decode takes one point's whole chain
-        // (about 4 ms) whatever its size, and rounds run one after another on
-        // the copy stream, so a new round is admitted only once the previous
-        // one has been published: requests that arrive meanwhile join it.
+        // (a few ms) whatever its size, so at most kDecStreams rounds are in
+        // flight, each on its own stream: requests that arrive while all are
+        // busy join the next round instead of queueing behind tiny ones.
         std::vector<Pending> admit;
         uint32_t room = ring.cap - (ring.pub - ring.tail);
-        const bool admitting = !(ring.h_comp && !ring.pub_pending.empty());
+        const bool admitting = !(ring.h_comp && ring.pub_pending.size() >= (size_t)Ring::kDecStreams);
         lk.lock();
         for (uint64_t tk : finished) done[tk] = t;
         items += finished_items;
@@ -370,11 +374,13 @@ struct bls_server {
         int rc = BLS_OK;
         if (ring.pub != from) {
             const uint32_t n = ring.pub - from;
-            if ((ring.h_comp ? (rc = ring_copy_in(ring.d_comp, ring.h_comp, 48, from, n)) || (rc = ring_decode(from, n))
-                             : (rc = ring_copy_in(ring.d_sigs, ring.h_sigs, 12, from, n))) ||
-                (rc = ring_copy_in(ring.d_nhms, ring.h_nhms, 12, from, n)) ||
-                (rc = ring_copy_in(ring.d_ids, ring.h_ids, 1, from, n)) ||
-                (rc = ring_copy_in(ring.d_res, ring.h_res, 1, from, n))) {
+            const cudaStream_t st = ring.h_comp ? ring.dec[ring.pub_round % Ring::kDecStreams] : ring.copy;
+            if ((ring.h_comp ? (rc = ring_copy_in(ring.d_comp, ring.h_comp, 48, from, n, st)) ||
+                                   (rc = ring_decode(from, n, st))
+                             : (rc = ring_copy_in(ring.d_sigs, ring.h_sigs, 12, from, n, st))) ||
+                (rc = ring_copy_in(ring.d_nhms, ring.h_nhms, 12, from, n, st)) ||
+                (rc = ring_copy_in(ring.d_ids, ring.h_ids, 1, from, n, st)) ||
+                (rc = ring_copy_in(ring.d_res, ring.h_res, 1, from, n, st))) {
                 lk.lock();
                 return rc;
             }
@@ -390,8 +396,11 @@ struct bls_server {
             }
             const int slot = (int)(ring.pub_round++ % Ring::kPubSlots);
             ring.h_pubv[slot] = ring.pub;
-            if (cudaMemcpyAsync(ring.d_ctl, ring.h_pubv + slot, 4, cudaMemcpyHostToDevice, ring.copy) ||
-                cudaEventRecord(ring.pub_ev[slot], ring.copy)) {
+            // counts land in order: a decode round's count after the round before it
+            if ((st != ring.copy && !ring.pub_pending.empty() &&
+                 cudaStreamWaitEvent(st, ring.pub_ev[ring.pub_pending.back().first], 0)) ||
+                cudaMemcpyAsync(ring.d_ctl, ring.h_pubv + slot, 4, cudaMemcpyHostToDevice, st) ||
+                cudaEventRecord(ring.pub_ev[slot], st)) {
                 lk.lock();
                 return BLS_ERR_CUDA;
             }
@@ -430,6 +439,8 @@ struct bls_server {
     void ring_stop() {
         if (!ring.h_ctl || !ring.d_ctl) return;
         ring.h_ctl[1] = 1;
+        for (cudaStream_t st : ring.dec)
+            if (st) cudaStreamSynchronize(st);
         cudaMemcpyAsync(ring.d_ctl + 1, ring.h_ctl + 1, 4, cudaMemcpyHostToDevice, ring.copy);
         cudaStreamSynchronize(ring.copy);
         if (ring.kern) cudaStreamSynchronize(ring.kern);
@@ -547,6 +558,8 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
                   cudaDeviceSynchronize() == cudaSuccess;
         for (int k = 0; ok && k < Ring::kPubSlots; ++k)
             ok = cudaEventCreateWithFlags(&r.pub_ev[k], cudaEventDisableTiming) == cudaSuccess;
+        for (int k = 0; ok && comp && k < Ring::kDecStreams; ++k)
+            ok = cudaStreamCreateWithFlags(&r.dec[k], cudaStreamNonBlocking) == cudaSuccess;
         if (ok) memset(r.h_ctl, 0, 64);
         if (!ok) {
             bls_server_destroy(s);
@@ -607,6 +620,8 @@ void bls_server_destroy(bls_server* s) {
         for (cudaEvent_t ev : r.pub_ev)
             if (ev) cudaEventDestroy(ev);
         if (r.poll) cudaStreamDestroy(r.poll);
+        for (cudaStream_t st : r.dec)
+            if (st) cudaStreamDestroy(st);
         for (void* p : {(void*)r.d_sigs, (void*)r.d_nhms, (void*)r.d_ids, (void*)r.d_res, (void*)r.d_ctl,
                         (void*)r.d_comp, (void*)r.d_st})
             if (p) cudaFree(p);
