@@ -62,6 +62,26 @@ __global__ void __launch_bounds__(128) k_g1_decompress(const uint8_t* in, int n,
     fp_store_u64(xy + 12 * (size_t)i + 6, y);
 }
 
+// The serving ring's decoder: the same decode, grid-stride, in blocks that
+// each hold a whole SM.  Its dynamic shared memory (unused) is more than half
+// of an SM's, so two of its blocks never share an SM and none shares one with
+// a resident ring-kernel block; a launch of b blocks therefore occupies at
+// most b SMs, where blocks of the plain decoder would spread over every SM
+// that frees up and keep the ring kernel's whole-SM blocks from starting.
+constexpr int kDecSmThreads = 384;
+constexpr size_t kDecSmSmem = 116 * 1024;
+__global__ void __launch_bounds__(kDecSmThreads, 1) k_g1_decompress_sm(const uint8_t* in, int n, uint64_t* xy,
+                                                                     int32_t* status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        fp x, y;
+        bool id;
+        const int32_t st = g1_decode(in + 48 * (size_t)i, x, y, id, true);
+        status[i] = st;
+        fp_store_u64(xy + 12 * (size_t)i, x);
+        fp_store_u64(xy + 12 * (size_t)i + 6, y);
+    }
+}
+
 // q: 24 x uint64 per key (x.c0, x.c1, y.c0, y.c1 Montgomery; zeros for the
 // identity and for a failure); identity (optional): 1 for the identity.
 __global__ void __launch_bounds__(64) k_g2_decompress(const uint8_t* in, int n, uint64_t* q, int32_t* status,
@@ -244,6 +264,19 @@ cudaError_t launch_verify(const VerifyArgs& a, cudaStream_t s) {
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     k_g1_decompress<<<(n + 127) / 128, 128, 0, s>>>(in, n, xy, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g1_decompress_sms(const uint8_t* in, int n, uint64_t* xy, int32_t* status, int max_sms,
+                                     cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        k_g1_decompress_sm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDecSmSmem);
+    if (attr != cudaSuccess) return attr;
+    int blocks = (n + kDecSmThreads - 1) / kDecSmThreads;
+    if (blocks > max_sms) blocks = max_sms;
+    if (blocks < 1) blocks = 1;
+    k_g1_decompress_sm<<<blocks, kDecSmThreads, kDecSmSmem, s>>>(in, n, xy, status);
     return cudaGetLastError();
 }
 

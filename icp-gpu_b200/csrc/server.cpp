@@ -124,14 +124,18 @@ struct Ring {
 };
 constexpr int32_t kSentinel = 0x7fffffff;
 // SMs left free of the twelve-warp ring kernel for the decoder of compressed
-// signatures (a block of the decoder does not fit beside a resident block).
-// The decoder takes one thread per point through a chain of about 1,300
-// multiplication-equivalents (the square root's 376 squarings and 85
-// products, the subgroup check's 127 doublings), a few ms, with three blocks
-// of 128 threads per SM.  The split balances the two rates: a verify costs
-// the ring kernel about 280 k SM-cycles and a decode about 28 k, so 14 of
-// 148 SMs decode (12 left the decoder the bottleneck of a saturated ring).
-constexpr int kDecodeSms = 14;
+// signatures.  The decoder takes one thread per point through a chain of
+// about 1,300 multiplication-equivalents (the square root's 376 squarings
+// and 85 products, the subgroup check's 127 doublings), about 2.3 ms, in
+// whole-SM blocks of 384 threads; each decode round (up to kDecStreams in
+// flight) takes at most kDecSmsPerRound SMs, so the decoder never holds more
+// than the SMs set aside for it and the ring kernel's blocks always find
+// theirs.  Three SMs retire about 1,150 points per 2.3 ms pass, 500 k/s, so
+// the four rounds keep the decoder well ahead of the other 136 SMs' verify
+// rate (about 7 k verifies/s per SM).
+constexpr int kDecSmsPerRound = 3;
+constexpr int kDecodeSms = Ring::kDecStreams * kDecSmsPerRound;
+constexpr int kDecRoundItems = kDecSmsPerRound * 384;   // one pass of a round's decoder blocks
 
 struct bls_server {
     bls_ctx* ctx = nullptr;
@@ -261,10 +265,11 @@ struct bls_server {
     // points into d_sigs, each slot's decode status into d_st
     int ring_decode(uint32_t a, uint32_t n, cudaStream_t st) {
         const uint32_t s0 = a % ring.cap, first = std::min(n, ring.cap - s0);
-        if (bls::launch_g1_decompress(ring.d_comp + 48 * (size_t)s0, (int)first, ring.d_sigs + 12 * (size_t)s0,
-                                      ring.d_st + s0, st))
+        if (bls::launch_g1_decompress_sms(ring.d_comp + 48 * (size_t)s0, (int)first, ring.d_sigs + 12 * (size_t)s0,
+                                          ring.d_st + s0, kDecSmsPerRound, st))
             return BLS_ERR_CUDA;
-        if (first < n && bls::launch_g1_decompress(ring.d_comp, (int)(n - first), ring.d_sigs, ring.d_st, st))
+        if (first < n && bls::launch_g1_decompress_sms(ring.d_comp, (int)(n - first), ring.d_sigs, ring.d_st,
+                                                       kDecSmsPerRound, st))
             return BLS_ERR_CUDA;
         return BLS_OK;
     }
@@ -331,9 +336,15 @@ struct bls_server {
         lk.lock();
         for (uint64_t tk : finished) done[tk] = t;
         items += finished_items;
+        uint32_t round_items = 0;
         while (admitting && !queue.empty()) {
             const uint32_t span = ((uint32_t)queue.front().n + ring.group - 1) / ring.group * ring.group;
             if (span > room) break;
+            // a decode round stays within one pass of its SMs (a larger request
+            // goes alone): rounds of whatever is queued would hold the ring's
+            // whole free space in a few long decodes while the verifier starves
+            if (ring.h_comp && round_items > 0 && round_items + span > (uint32_t)kDecRoundItems) break;
+            round_items += span;
             room -= span;
             if ((uint64_t)queue.front().n > max_batch) max_batch = queue.front().n;
             admit.push_back(std::move(queue.front()));
