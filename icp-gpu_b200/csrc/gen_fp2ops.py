@@ -478,12 +478,14 @@ PROGRAMS = [
 X_ABS = 0xd201000000010000
 OP_LOAD_CORR, OP_MILLER_DONE, OP_LOAD_LINES = 29, 30, 31
 COND_ML = 1 << 21     # op runs only when the Miller value is wanted
+NO_WAR = 1 << 22      # the op's program writes no slot it reads (set by encode_op)
 T_GROUP = 3       # the inverse's temporaries start at group 3's slot 0
+PHYS_GROUPS = 7   # Fp12 groups of the item area: one more than the final exponentiation's live values
 
 
-def driver_sequence(normalised=False):
-    """The op sequence of one verification; `normalised`: the line tables are
-    divided by their c2 (LINE1N / LINE2N)."""
+def logical_sequence(normalised=False):
+    """The op sequence of one verification over six logical Fp12 groups;
+    `normalised`: the line tables are divided by their c2 (LINE1N / LINE2N)."""
     pid = {name: i for i, (name, _, _) in enumerate(PROGRAMS)}
     seq = []
     l1, l2 = ("LINE1N", "LINE2N") if normalised else ("LINE1", "LINE2")
@@ -549,6 +551,121 @@ def driver_sequence(normalised=False):
     return seq
 
 
+def driver_sequence(normalised=False):
+    """The op sequence of one verification as the kernels run it: the groups
+    placed by place_groups; Gt ends in group gt_group(normalised)."""
+    return place_groups(logical_sequence(normalised))[0]
+
+
+def gt_group(normalised=False):
+    """the physical group that holds Gt after driver_sequence(normalised)"""
+    return place_groups(logical_sequence(normalised))[1]
+
+
+def program_io(code):
+    """(bases read, bases written) of program `code`"""
+    reads, writes = set(), set()
+    for o in PROGRAMS[code][1]():
+        if o is None:
+            continue
+        writes.add(o.dst >> 4)
+        reads.update(r >> 4 for t in o.terms for r in (t.x, t.y) if r is not None)
+        reads.update(r >> 4 for _, r in o.lins)
+    return reads, writes
+
+
+def live_after(seq):
+    """per op, the logical groups a later op still reads (the final value,
+    group 0, counts as read at the end; ops that run only when the Miller
+    value is wanted read but never end a value's life)"""
+    n_prog = len(PROGRAMS)
+    out = [None] * len(seq)
+    cur = {0}
+    for i in range(len(seq) - 1, -1, -1):
+        code, d, a, b, _ = seq[i]
+        c = code & ~COND_ML
+        out[i] = set(cur)
+        if c == OP_MILLER_DONE:
+            cur.add(d)
+            continue
+        if c >= n_prog:
+            continue
+        rb, wb = program_io(c)
+        if B_D in wb and not code & COND_ML:
+            cur.discard(d)
+        if B_A in rb:
+            cur.add(a)
+        if B_B in rb:
+            cur.add(b)
+    return out
+
+
+def place_groups(seq):
+    """Put the sequence's Fp12 values (logical groups 0..5) into PHYS_GROUPS
+    physical groups so that as few programs as possible write a group they
+    read: a result that would overwrite one of its operands (f = f^2,
+    f = f * x) goes to a group whose value no later op reads, when there is
+    one, and the value moves there.  Such a program writes only slots that
+    none of its outputs reads, which lets the kernel store each output as
+    soon as it is reduced (no block barrier between the reads and the
+    stores; the op's NO_WAR flag).  Parts of the final exponentiation hold
+    six live values, so with seven groups there is always one: every
+    program of both sequences is out of place, which the 32-item kernel
+    relies on (emit refuses a sequence where one is not).  Returns the placed
+    sequence and the physical group of the final value (Gt)."""
+    n_prog = len(PROGRAMS)
+    live = live_after(seq)
+    m = {0: 0}                             # logical group -> physical group (f = 1 starts in group 0)
+    out = []
+    for i, (code, d, a, b, ci) in enumerate(seq):
+        c = code & ~COND_ML
+        if c < n_prog:
+            rb, wb = program_io(c)
+            pa = m[a] if B_A in rb else 0
+            pb = m[b] if B_B in rb else 0
+            if B_D in wb:
+                srcs = ({pa} if B_A in rb else set()) | ({pb} if B_B in rb else set())
+                busy = {m[x] for x in live[i] if x != d and x in m} | srcs
+                if d not in m or m[d] in busy:
+                    free = [g for g in range(PHYS_GROUPS) if g not in busy]
+                    m[d] = free[0] if free else m[d]
+            out.append((code, m[d] if B_D in wb else 0, pa, pb, ci))
+        elif c == OP_MILLER_DONE:
+            out.append((code, m[d], a, b, ci))
+        else:
+            out.append((code, d, a, b, ci))
+    return out, m[0]
+
+
+def op_slots(op):
+    """(slots read, slots written) of a program op, as (space, index) pairs:
+    space 'g' is the item's group area (6 slots per group), 'c' the C area,
+    'k' the constant slots"""
+    code, d, a, b, ci = op
+    code &= ~COND_ML
+    base = {B_D: ("g", 6 * d), B_A: ("g", 6 * a), B_B: ("g", 6 * b), B_C: ("c", 0), B_K: ("k", 0),
+            B_T: ("g", 6 * T_GROUP)}
+    rd, wr = set(), set()
+    for o in PROGRAMS[code][1]():
+        if o is None:
+            continue
+        sp, off = base[o.dst >> 4]
+        wr.add((sp, off + (o.dst & 15)))
+        for r in [r for t in o.terms for r in (t.x, t.y) if r is not None] + [r for _, r in o.lins]:
+            sp, off = base[r >> 4]
+            rd.add((sp, off + (r & 15)))
+    return rd, wr
+
+
+def no_war(op):
+    """the op writes no slot that any of its outputs reads"""
+    code = op[0] & ~COND_ML
+    if code >= len(PROGRAMS):
+        return False
+    rd, wr = op_slots(op)
+    return not (rd & wr)
+
+
 def t_slots_used():
     """Temporary slots (base T) any program reads or writes."""
     hi = -1
@@ -584,7 +701,7 @@ def encode_op(op):
     cond = code & COND_ML
     code &= ~COND_ML
     assert code < 32 and d < 8 and a < 8 and b < 8 and ci < 128
-    return code | (d << 5) | (a << 8) | (b << 11) | (ci << 14) | cond
+    return code | (d << 5) | (a << 8) | (b << 11) | (ci << 14) | cond | (NO_WAR if no_war(op) else 0)
 
 
 def build():
@@ -817,14 +934,21 @@ def emit(path):
     L.append("// value is wanted; kOpMillerDone emits group D")
     L.append("constexpr uint32_t kOpLoadCorr = %d, kOpMillerDone = %d, kOpLoadLines = %d, kCondMl = 0x%xu;"
              % (OP_LOAD_CORR, OP_MILLER_DONE, OP_LOAD_LINES, COND_ML))
+    L.append("// kNoWar: the program writes no slot that any of its outputs reads, so its stores need")
+    L.append("// no block barrier after the reads")
+    L.append("constexpr uint32_t kNoWar = 0x%xu;" % NO_WAR)
     L.append("constexpr int kTGroup = %d;" % T_GROUP)
     max_bias = max(b for name, fn, _ in PROGRAMS for o in fn() if o is not None
                    for b in (o.bias_re, o.bias_im, o.bias_lin_re, o.bias_lin_im))
     L.append("// largest bias multiple k of any output (the kernel keeps k p for k = 0 .. kMaxBias)")
     L.append("constexpr int kMaxBias = %d;" % max_bias)
     seqs = [driver_sequence(False), driver_sequence(True)]
+    for seq in seqs:   # verify_w.cu stores a program's outputs without a barrier after its reads
+        assert all(no_war(op) for op in seq if (op[0] & ~COND_ML) < len(PROGRAMS))
     L.append("// Fp12 groups the sequences touch (operands, results, the inverse's temporaries)")
     L.append("constexpr int kGroupsUsed = %d;" % groups_used(seqs))
+    L.append("// the group that holds Gt at the end of each sequence (raw, normalised)")
+    L.append("__device__ __constant__ uint32_t kGtGroup[2] = {%d, %d};" % (gt_group(False), gt_group(True)))
     n = max(len(q) for q in seqs)
     L.append("constexpr int kSeqLenRaw = %d, kSeqLenNorm = %d;" % (len(seqs[0]), len(seqs[1])))
     L.append("__device__ __constant__ uint32_t kSeq[2][%d] = {" % n)

@@ -59,16 +59,16 @@ struct Ctx {
     bool active;       // thread belongs to a pairing
 };
 
-// D, A, B, C, K, T: absolute slot of index 0, one byte each (every slot index
-// of a block is below 256), so a reference resolves with a shift, not an
-// indexed array
+// D, A, B, C, K, T: absolute slot of index 0, nine bits each (every slot
+// index of a block is below 512), so a reference resolves with a shift, not
+// an indexed array
 struct Bases { uint64_t b; };
-static_assert(kKSlots + kPairsPerBlock * kPairSlots <= 256, "slot indices must fit a byte");
+static_assert(kKSlots + kPairsPerBlock * kPairSlots <= 512, "slot indices must fit nine bits");
 
 __device__ __forceinline__ uint32_t grp(const Ctx& c, int g) { return c.region + 6 * g; }
 
 __device__ __forceinline__ uint32_t slot_addr(const Bases& bs, uint32_t ref) {
-    return (uint32_t)(bs.b >> (8u * (ref >> 4))) % 256u + (ref & 15u);
+    return (uint32_t)(bs.b >> (9u * (ref >> 4))) % 512u + (ref & 15u);
 }
 
 __device__ __forceinline__ void load_fp(uint32_t* x, const uint32_t* sm, uint32_t slot, int comp) {
@@ -531,13 +531,13 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
                 if (a.ml_out) emit_group(c, (e >> 5) & 7u, have ? a.ml_out + 72 * (size_t)item : nullptr);
             } else {
                 Bases bs;
-                bs.b = (uint64_t)grp(c, (e >> 5) & 7u) | (uint64_t)grp(c, (e >> 8) & 7u) << 8 |
-                       (uint64_t)grp(c, (e >> 11) & 7u) << 16 | (uint64_t)(c.region + kCOff) << 24 |
-                       (uint64_t)grp(c, f2::kTGroup) << 40;
+                bs.b = (uint64_t)grp(c, (e >> 5) & 7u) | (uint64_t)grp(c, (e >> 8) & 7u) << 9 |
+                       (uint64_t)grp(c, (e >> 11) & 7u) << 18 | (uint64_t)(c.region + kCOff) << 27 |
+                       (uint64_t)grp(c, f2::kTGroup) << 45;
                 run((int)code, sm, c.pair, c.lane, c.half, bs);
             }
         }
-        const bool one = emit_group(c, 0, (have && a.gt_out) ? a.gt_out + 72 * (size_t)item : nullptr);
+        const bool one = emit_group(c, (int)f2::kGtGroup[norm], (have && a.gt_out) ? a.gt_out + 72 * (size_t)item : nullptr);
         if (have && c.lane == 0 && c.half == 0) a.results[item] = status != 0 ? -status : (one ? 1 : 0);
         __syncthreads();
     }

@@ -279,7 +279,11 @@ __device__ __forceinline__ void finish(uint32_t off, const Sm& s, const Bases& b
 
 // program `pid` for every item of the block: accumulate, exchange (the two
 // warps of coefficient k meet), reduce, meet, write, meet.  The descriptor
-// index of the role is 8 half + k.
+// index of the role is 8 half + k.  No program of the generated sequences
+// writes a slot that any role of it reads (the generator places a result
+// that would overwrite an operand in an unused group, and refuses to emit a
+// sequence where it cannot), so a role stores its output as soon as it has
+// it: one block-wide meeting per program, after the stores.
 __device__ __forceinline__ void run(int pid, const Sm& s, int k, int half, const Bases& bs) {
     const uint32_t off = f2::kOutIndex[pid][8 * half + k];
     const uint32_t mode = off != 0xffffu ? (f2::kDesc[off] & 3u) : 0u;
@@ -294,7 +298,6 @@ __device__ __forceinline__ void run(int pid, const Sm& s, int k, int half, const
     asm volatile("bar.sync %0, 64;" ::"r"(1 + k) : "memory");
     uint32_t o[12];
     if (off != 0xffffu) finish(off, s, bs, half, own, theirs, o);
-    __syncthreads();
     if (off != 0xffffu) store_fp(s, slot_addr(bs, (f2::kDesc[off] >> 8) & 0x7fu), half, o);
     __syncthreads();
 }
@@ -564,7 +567,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_verify_w(VerifyArgs a, const ui
                 run((int)code, s, k, half, bs);
             }
         }
-        const bool one = emit_group(s, 0, k, half, (have && a.gt_out) ? a.gt_out + 72 * (size_t)item : nullptr);
+        const bool one = emit_group(s, (int)f2::kGtGroup[norm], k, half,
+                                    (have && a.gt_out) ? a.gt_out + 72 * (size_t)item : nullptr);
         if (have && role == 0) {
             const int32_t status = (int32_t)info[2];
             a.results[item] = status != 0 ? -status : (one ? 1 : 0);

@@ -140,5 +140,5 @@ def verify(sig, nhm, g2_limbs, pk_limbs, skip1=False, skip2=False, normalised=Fa
             ml = [v * B.MONT_RINV % B.P for v in m.group_flat(d)]
         else:
             m.call(names[code], d, a, b)
-    gt = [v * B.MONT_RINV % B.P for v in m.group_flat(0)]
+    gt = [v * B.MONT_RINV % B.P for v in m.group_flat(G.gt_group(normalised))]
     return ml, gt

@@ -84,9 +84,73 @@ def test_wide_kernel_layout_fits_one_block_per_sm():
     slot_u4 = item_slots * 6 * v
     k_u4 = k_slots * 6
     xch_u4 = 6 * 2 * 7 * v
+    qp_u4 = 128 * 4
     kp = (17 + 1) * 64
-    total = (slot_u4 + k_u4 + xch_u4) * 16 + kp + 4 * v * 4 + 16 * v + 16
+    total = (slot_u4 + k_u4 + xch_u4 + qp_u4) * 16 + kp + 4 * v * 4 + 16 * v + 16
     assert total <= 227 * 1024
     src = open(os.path.join(CSRC, "verify_w.cu")).read()
-    for name in ("kItemSlots = kCOff + 12", "kSlotU4 = kItemSlots * 6 * kV", "kXchU4 = 6 * 2 * 7 * kV"):
+    for name in ("kItemSlots = kCOff + 12", "kSlotU4 = kItemSlots * 6 * kV", "kXchU4 = 6 * 2 * 7 * kV",
+                 "kQpU4 = 128 * 4"):
         assert name in src
+
+
+def test_every_program_writes_no_slot_it_reads():
+    """The generator sends every result that would overwrite an operand to a
+    group whose value is dead; the final exponentiation holds at most six
+    live values, so with seven groups one is always free.  No program of
+    either sequence then writes a slot that one of its outputs reads, which
+    the 32-item kernel relies on when it stores a program's outputs without
+    a block barrier after the reads; each op's word carries the flag."""
+    n_prog = len(G.PROGRAMS)
+    for normalised in (False, True):
+        logical = G.logical_sequence(normalised)
+        live = G.live_after(logical)
+        busiest = 0
+        progs = 0
+        for i, op in enumerate(G.driver_sequence(normalised)):
+            if (op[0] & ~G.COND_ML) >= n_prog:
+                assert not G.encode_op(op) & G.NO_WAR
+                continue
+            rd, wr = G.op_slots(op)
+            assert not (rd & wr), op
+            assert G.encode_op(op) & G.NO_WAR
+            code, d, a, b, _ = logical[i]
+            rb, _ = G.program_io(code & ~G.COND_ML)
+            srcs = ({a} if G.B_A in rb else set()) | ({b} if G.B_B in rb else set())
+            busiest = max(busiest, len((live[i] - {d}) | srcs))
+            progs += 1
+        assert progs > 640 and busiest < G.PHYS_GROUPS
+
+
+def test_inverse_temporaries_hold_no_live_value():
+    """The inverse's temporaries (base T, from group kTGroup) overwrite only
+    groups whose values are dead: walking each sequence backwards from the
+    final read of Gt, no group that a later op still reads lies under a slot
+    an inverse program writes (ops that run only when the Miller value is
+    wanted count as readers but never as writers)."""
+    n_prog = len(G.PROGRAMS)
+    for normalised in (False, True):
+        seq = G.driver_sequence(normalised)
+        live = {G.gt_group(normalised)}
+        checked = 0
+        for op in reversed(seq):
+            code, d, a, b, _ = op
+            c = code & ~G.COND_ML
+            if c == G.OP_MILLER_DONE:
+                live.add(d)
+                continue
+            if c >= n_prog:
+                continue
+            rb, wb = G.program_io(c)
+            if G.B_T in wb:
+                t_groups = {G.T_GROUP + (o.dst & 15) // 6 for o in G.PROGRAMS[c][1]() if o is not None
+                            and (o.dst >> 4) == G.B_T}
+                assert not (t_groups & live), (G.PROGRAMS[c][0], t_groups, live)
+                checked += 1
+            if G.B_D in wb and not code & G.COND_ML:
+                live.discard(d)
+            if G.B_A in rb:
+                live.add(a)
+            if G.B_B in rb:
+                live.add(b)
+        assert checked == 7
