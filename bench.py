@@ -60,7 +60,7 @@ IMAD_PER_FP_MUL = 588   # the reference CIOS multiply: 12 rows x (24 for a b_i +
 ALGO_IMAD_PER_VERIFY = ALGO_FP_MULS_PER_VERIFY * IMAD_PER_FP_MUL
 # DRAM bytes of one 4,096-verify launch of the verify kernel (k_verify_w),
 # measured with ncu (1.76 MB read, 0 written): the kernel is not memory-bound.
-DRAM_BYTES_PER_LAUNCH = 1763072
+DRAM_BYTES_PER_LAUNCH = 1762560
 
 
 def dist_env():
