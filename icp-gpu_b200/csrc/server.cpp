@@ -262,15 +262,23 @@ struct bls_server {
     }
 
     // decode ring range [a, a + n) (may wrap) on stream st: the decoded
-    // points into d_sigs, each slot's decode status into d_st
+    // points into d_sigs, each slot's decode status into d_st.  Beside the
+    // twelve-warp kernel, which leaves kDecodeSms SMs empty, the decoder runs
+    // in whole-SM blocks, at most kDecSmsPerRound of them; the five-item
+    // kernel's small blocks fill every SM but leave room for the plain
+    // decoder's 128-thread blocks beside them, where a whole-SM block would
+    // wait for the ring kernel to go idle.
     int ring_decode(uint32_t a, uint32_t n, cudaStream_t st) {
         const uint32_t s0 = a % ring.cap, first = std::min(n, ring.cap - s0);
-        if (bls::launch_g1_decompress_sms(ring.d_comp + 48 * (size_t)s0, (int)first, ring.d_sigs + 12 * (size_t)s0,
-                                          ring.d_st + s0, kDecSmsPerRound, st))
-            return BLS_ERR_CUDA;
-        if (first < n && bls::launch_g1_decompress_sms(ring.d_comp, (int)(n - first), ring.d_sigs, ring.d_st,
-                                                       kDecSmsPerRound, st))
-            return BLS_ERR_CUDA;
+        auto decode = [&](uint32_t from, uint32_t count) {
+            return view.shape == bls::kShapeWide
+                       ? bls::launch_g1_decompress_sms(ring.d_comp + 48 * (size_t)from, (int)count,
+                                                       ring.d_sigs + 12 * (size_t)from, ring.d_st + from,
+                                                       kDecSmsPerRound, st)
+                       : bls::launch_g1_decompress(ring.d_comp + 48 * (size_t)from, (int)count,
+                                                   ring.d_sigs + 12 * (size_t)from, ring.d_st + from, st);
+        };
+        if (decode(s0, first) || (first < n && decode(0, n - first))) return BLS_ERR_CUDA;
         return BLS_OK;
     }
 
