@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -1162,6 +1163,85 @@ int bls_g1_decompress_status(bls_ctx* ctx, const uint8_t* in, int n, uint64_t* x
 
 // --------------------------------------------------------------- reference ABI
 
+namespace {
+
+// The reference entry point's repeat call over tables it has seen before
+// (the common case: a batch of shares over a few registered keys), with the
+// host's exact table check moved off the critical path.  The items are
+// grouped by table fingerprint, each group's first table is found (by exact
+// content) among the registered keys or registered, and the verify launches
+// with those key ids at once; while it runs, the host compares every item's
+// whole table with its group's first one.  The results are returned only if
+// every table matched; otherwise (two different tables with one fingerprint)
+// *done stays false and the caller runs the exact path, which decides every
+// item's table by full comparison before launching.  Also *done = false when
+// the caller's generator table is not the context's, when most tables are
+// distinct, or when the key store is full.
+int verify_cached_speculative(bls_ctx* c, const uint64_t* sigs, const uint64_t* neg_hms, const uint64_t* g2_coeffs,
+                              const uint64_t* pk_coeffs, int M, int32_t* results, bool* done) {
+    *done = false;
+    const size_t n = (size_t)M, W = bls::kCoeffU64;
+    if (c->h_g2_table.empty()) {
+        c->h_g2_table.resize(W);
+        CK(cudaMemcpyAsync(c->h_g2_table.data(), c->d_g2, W * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (memcmp(g2_coeffs, c->h_g2_table.data(), W * 8) != 0) return BLS_OK;
+    std::vector<uint64_t> fp(n);
+    host_parallel_for(M, [&](int i) { fp[i] = table_fingerprint(pk_coeffs + W * (size_t)i); });
+    std::vector<int32_t> group(n);
+    std::vector<int> first_item;
+    std::unordered_map<uint64_t, int32_t> of_fp;
+    of_fp.reserve(64);
+    for (size_t i = 0; i < n; ++i) {
+        auto it = of_fp.emplace(fp[i], (int32_t)first_item.size());
+        if (it.second) first_item.push_back((int)i);
+        group[i] = it.first->second;
+    }
+    if (2 * first_item.size() > n) return BLS_OK;
+    std::vector<const uint64_t*> tables(first_item.size());
+    for (size_t j = 0; j < first_item.size(); ++j) tables[j] = pk_coeffs + W * (size_t)first_item[j];
+    std::vector<int32_t> ids;
+    int rc;
+    if (!cached_table_ids(c, tables, ids, &rc)) return rc;
+    if (rc) return rc;
+    if ((rc = c->grow(c->d_sigs, n * 96)) || (rc = c->grow(c->d_nhms, n * 96)) || (rc = c->grow(c->d_pkidx, n * 4)) ||
+        (rc = c->grow(c->d_res, n * 4)) || (rc = c->grow(c->h_pkidx, n * 4)) || (rc = c->grow(c->h_res, n * 4)))
+        return rc;
+    int32_t* hidx = (int32_t*)c->h_pkidx.p;
+    for (size_t i = 0; i < n; ++i) hidx[i] = ids[group[i]];
+    CK(cudaMemcpyAsync(c->d_sigs.p, sigs, n * 96, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_nhms.p, neg_hms, n * 96, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_pkidx.p, hidx, n * 4, cudaMemcpyHostToDevice, c->stream));
+    bls::VerifyArgs a{};
+    a.sigs = c->d_sigs.p;
+    a.sig_compressed = 0;
+    a.nhms = (const uint64_t*)c->d_nhms.p;
+    a.g2 = c->d_g2;
+    a.pk_tables = c->d_pk;
+    c->set_norm(a);
+    a.pk_index = (const int32_t*)c->d_pkidx.p;
+    a.pk_identity = c->d_pk_inf;
+    a.n = M;
+    a.results = (int32_t*)c->d_res.p;
+    if ((rc = run_verify(c, a))) return rc;
+    CK(cudaMemcpyAsync(c->h_res.p, a.results, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    // the exact check, while the GPU verifies
+    std::atomic<bool> same{true};
+    host_parallel_for(M, [&](int i) {
+        if ((size_t)i != (size_t)first_item[group[i]] &&
+            memcmp(pk_coeffs + W * (size_t)i, tables[group[i]], W * 8) != 0)
+            same.store(false, std::memory_order_relaxed);
+    });
+    CK(cudaStreamSynchronize(c->stream));
+    if (!same.load()) return BLS_OK;
+    memcpy(results, c->h_res.p, n * 4);
+    *done = true;
+    return BLS_OK;
+}
+
+}  // namespace
+
 int gpu_crypto_init(void) {
     bls_ctx* c;
     return default_ctx(&c) == BLS_OK ? 0 : -1;
@@ -1181,6 +1261,9 @@ int gpu_batch_bls_verify(const uint64_t* sigs, const uint64_t* neg_hms, const ui
         CK(cudaSetDevice(c->cfg.device));
         size_t n = (size_t)M;
         const size_t W = bls::kCoeffU64;
+        bool done = false;
+        if (int rc0 = verify_cached_speculative(c, sigs, neg_hms, g2_coeffs, pk_coeffs, M, results, &done)) return rc0;
+        if (done) return BLS_OK;
         // repeated keys: only the distinct tables cross, with an item -> table
         // index; mostly distinct tables cross whole (no index)
         std::vector<int32_t> idx;
