@@ -275,9 +275,12 @@ __device__ __forceinline__ void finish(uint32_t off, const uint32_t* sm, const B
     f2::qp_reduce(o, r);
 }
 
-// run program `pid` on the pairing: accumulate, exchange, meet, reduce, meet,
-// write, meet.  Every thread of the block takes part in every barrier.  It has
-// one call site (the op loop of the kernel), so it is inlined there.
+// run program `pid` on the pairing: accumulate, exchange, meet, reduce,
+// write, meet.  No program of the generated sequences writes a slot that it
+// reads (gen_fp2ops.py places the results), so the outputs are stored as soon
+// as they are reduced.  Every thread of the block takes part in every
+// barrier.  It has one call site (the op loop of the kernel), so it is
+// inlined there.
 __device__ __forceinline__ void run(int pid, uint32_t* sm, int pair, int lane, int half, const Bases& bs) {
     const bool active = pair < kPairsPerBlock;
     const uint32_t off = active ? f2::kOutIndex[pid][8 * half + lane] : 0xffffu;
@@ -289,7 +292,6 @@ __device__ __forceinline__ void run(int pid, uint32_t* sm, int pair, int lane, i
     __syncthreads();
     uint32_t o[12];
     if (off != 0xffffu) finish(off, sm, bs, half, own, xch + kXchWords * (1 - half), o);
-    __syncthreads();
     if (off != 0xffffu) store_fp(sm, slot_addr(bs, (f2::kDesc[off] >> 8) & 0x7fu), half, o);
     __syncthreads();
 }
