@@ -70,9 +70,14 @@ cudaError_t launch_rlc(const RlcArgs& a, cudaStream_t s);
 cudaError_t launch_gt_product(uint64_t* gt, int n, int* counters, cudaStream_t s);
 cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t* status, cudaStream_t s);
 // the same decode in whole-SM blocks, at most max_sms of them (grid-stride):
-// the serving ring's decoder, which must stay within the SMs left to it
+// the serving ring's decoder, which must stay within the SMs left to it;
+// check_subgroup false leaves the subgroup test to launch_g1_subgroup_sms
 cudaError_t launch_g1_decompress_sms(const uint8_t* in, int n, uint64_t* xy, int32_t* status, int max_sms,
-                                     cudaStream_t s);
+                                     bool check_subgroup, cudaStream_t s);
+// sub[i] = ST_NOT_IN_SUBGROUP (4) for a decoded point (status 0, not the
+// identity) outside G1, else 0; whole-SM blocks, at most max_sms
+cudaError_t launch_g1_subgroup_sms(const uint64_t* xy, const int32_t* status, int n, int32_t* sub, int max_sms,
+                                   cudaStream_t s);
 cudaError_t launch_neg_hash_to_g1(const uint8_t* msgs, const uint32_t* offsets, int n, const uint8_t* dst,
                                   int dst_len, uint64_t* out, cudaStream_t s);
 cudaError_t launch_g2_decompress(const uint8_t* in, int n, uint64_t* q, int32_t* status, uint8_t* identity,

@@ -70,15 +70,32 @@ __global__ void __launch_bounds__(128) k_g1_decompress(const uint8_t* in, int n,
 // that frees up and keep the ring kernel's whole-SM blocks from starting.
 constexpr int kDecSmThreads = 384;
 constexpr size_t kDecSmSmem = 116 * 1024;
+// check_subgroup false: every check but the subgroup test, which
+// k_g1_subgroup_sm then runs over the decoded points.
 __global__ void __launch_bounds__(kDecSmThreads, 1) k_g1_decompress_sm(const uint8_t* in, int n, uint64_t* xy,
-                                                                     int32_t* status) {
+                                                                     int32_t* status, bool check_subgroup) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         fp x, y;
         bool id;
-        const int32_t st = g1_decode(in + 48 * (size_t)i, x, y, id, true);
+        const int32_t st = g1_decode(in + 48 * (size_t)i, x, y, id, check_subgroup);
         status[i] = st;
         fp_store_u64(xy + 12 * (size_t)i, x);
         fp_store_u64(xy + 12 * (size_t)i + 6, y);
+    }
+}
+
+// The subgroup test of points decoded without it, in the same whole-SM
+// blocks: sub[i] = ST_NOT_IN_SUBGROUP for a point outside G1, else 0 (also
+// for a point whose decode failed, or the identity).
+__global__ void __launch_bounds__(kDecSmThreads, 1) k_g1_subgroup_sm(const uint64_t* xy, const int32_t* status, int n,
+                                                                   int32_t* sub) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int32_t r = 0;
+        if (status[i] == ST_OK) {
+            const fp x = fp_load_u64(xy + 12 * (size_t)i), y = fp_load_u64(xy + 12 * (size_t)i + 6);
+            if (!g1_limbs_identity(x, y) && !g1_in_subgroup(x, y)) r = ST_NOT_IN_SUBGROUP;
+        }
+        sub[i] = r;
     }
 }
 
@@ -267,16 +284,30 @@ cudaError_t launch_g1_decompress(const uint8_t* in, int n, uint64_t* xy, int32_t
     return cudaGetLastError();
 }
 
+static int dec_sm_blocks(int n, int max_sms) {
+    int blocks = (n + kDecSmThreads - 1) / kDecSmThreads;
+    if (blocks > max_sms) blocks = max_sms;
+    return blocks < 1 ? 1 : blocks;
+}
+
 cudaError_t launch_g1_decompress_sms(const uint8_t* in, int n, uint64_t* xy, int32_t* status, int max_sms,
-                                     cudaStream_t s) {
+                                     bool check_subgroup, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     static const cudaError_t attr = cudaFuncSetAttribute(
         k_g1_decompress_sm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDecSmSmem);
     if (attr != cudaSuccess) return attr;
-    int blocks = (n + kDecSmThreads - 1) / kDecSmThreads;
-    if (blocks > max_sms) blocks = max_sms;
-    if (blocks < 1) blocks = 1;
-    k_g1_decompress_sm<<<blocks, kDecSmThreads, kDecSmSmem, s>>>(in, n, xy, status);
+    k_g1_decompress_sm<<<dec_sm_blocks(n, max_sms), kDecSmThreads, kDecSmSmem, s>>>(in, n, xy, status,
+                                                                                  check_subgroup);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g1_subgroup_sms(const uint64_t* xy, const int32_t* status, int n, int32_t* sub, int max_sms,
+                                   cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        k_g1_subgroup_sm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDecSmSmem);
+    if (attr != cudaSuccess) return attr;
+    k_g1_subgroup_sm<<<dec_sm_blocks(n, max_sms), kDecSmThreads, kDecSmSmem, s>>>(xy, status, n, sub);
     return cudaGetLastError();
 }
 

@@ -95,8 +95,16 @@ struct Ring {
     // before it, so the published count only ever covers decoded slots
     static constexpr int kDecStreams = 4;
     cudaStream_t dec[kDecStreams] = {};
+    cudaEvent_t dec_idle[kDecStreams] = {};   // recorded after a round's last decode work
     uint8_t *h_comp = nullptr, *d_comp = nullptr;
     int32_t* d_st = nullptr;
+    // split decode (beside the twelve-warp kernel): a round is published once
+    // its points are decoded and checked but for the subgroup test, which
+    // then runs on the decoder's SMs while the kernel verifies; its outcome
+    // per slot (0, or 4 for a point outside G1, kSentinel until known) comes
+    // back beside the results and overrides a verify result
+    bool split = false;
+    int32_t *h_sub = nullptr, *d_sub = nullptr;
     uint64_t *d_sigs = nullptr, *d_nhms = nullptr;
     int32_t *d_ids = nullptr, *d_res = nullptr;
     uint32_t* d_ctl = nullptr;             // device: [0] published, [1] stop, [2] claimed
@@ -274,11 +282,22 @@ struct bls_server {
             return view.shape == bls::kShapeWide
                        ? bls::launch_g1_decompress_sms(ring.d_comp + 48 * (size_t)from, (int)count,
                                                        ring.d_sigs + 12 * (size_t)from, ring.d_st + from,
-                                                       kDecSmsPerRound, st)
+                                                       kDecSmsPerRound, !ring.split, st)
                        : bls::launch_g1_decompress(ring.d_comp + 48 * (size_t)from, (int)count,
                                                    ring.d_sigs + 12 * (size_t)from, ring.d_st + from, st);
         };
         if (decode(s0, first) || (first < n && decode(0, n - first))) return BLS_ERR_CUDA;
+        return BLS_OK;
+    }
+
+    // the subgroup test of ring range [a, a + n) (split decode), on stream st
+    int ring_subgroup(uint32_t a, uint32_t n, cudaStream_t st) {
+        const uint32_t s0 = a % ring.cap, first = std::min(n, ring.cap - s0);
+        auto check = [&](uint32_t from, uint32_t count) {
+            return bls::launch_g1_subgroup_sms(ring.d_sigs + 12 * (size_t)from, ring.d_st + from, (int)count,
+                                               ring.d_sub + from, kDecSmsPerRound, st);
+        };
+        if (check(s0, first) || (first < n && check(0, n - first))) return BLS_ERR_CUDA;
         return BLS_OK;
     }
 
@@ -307,6 +326,11 @@ struct bls_server {
                                 ring.poll) ||
                 (first < inflight && cudaMemcpyAsync(ring.h_res, ring.d_res, 4 * (size_t)(inflight - first),
                                                      cudaMemcpyDeviceToHost, ring.poll)) ||
+                (ring.split &&
+                 (cudaMemcpyAsync(ring.h_sub + s0, ring.d_sub + s0, 4 * (size_t)first, cudaMemcpyDeviceToHost,
+                                  ring.poll) ||
+                  (first < inflight && cudaMemcpyAsync(ring.h_sub, ring.d_sub, 4 * (size_t)(inflight - first),
+                                                       cudaMemcpyDeviceToHost, ring.poll)))) ||
                 cudaStreamSynchronize(ring.poll)) {
                 lk.lock();
                 return BLS_ERR_CUDA;
@@ -318,13 +342,18 @@ struct bls_server {
         for (auto& f : ring.flights) {
             if (f.complete) continue;
             bool all = true;
-            for (uint32_t k = f.span; k-- > 0;)
-                if (ring.h_res[(f.start + k) % ring.cap] == kSentinel) {
+            for (uint32_t k = f.span; k-- > 0;) {
+                const uint32_t slot = (f.start + k) % ring.cap;
+                if (ring.h_res[slot] == kSentinel || (ring.split && ring.h_sub[slot] == kSentinel)) {
                     all = false;
                     break;
                 }
+            }
             if (!all) continue;
-            for (int k = 0; k < f.req.n; ++k) f.req.results[k] = ring.h_res[(f.start + k) % ring.cap];
+            for (int k = 0; k < f.req.n; ++k) {
+                const uint32_t slot = (f.start + k) % ring.cap;
+                f.req.results[k] = ring.split && ring.h_sub[slot] != 0 ? -ring.h_sub[slot] : ring.h_res[slot];
+            }
             finished.push_back(f.req.ticket);
             finished_items += f.req.n;
             f.complete = true;
@@ -340,7 +369,15 @@ struct bls_server {
         // busy join the next round instead of queueing behind tiny ones.
         std::vector<Pending> admit;
         uint32_t room = ring.cap - (ring.pub - ring.tail);
-        const bool admitting = !(ring.h_comp && ring.pub_pending.size() >= (size_t)Ring::kDecStreams);
+        bool admitting = !(ring.h_comp && ring.pub_pending.size() >= (size_t)Ring::kDecStreams);
+        if (admitting && ring.split) {   // the next round's stream has finished its last round's subgroup test
+            const cudaError_t q = cudaEventQuery(ring.dec_idle[ring.pub_round % Ring::kDecStreams]);
+            if (q != cudaSuccess && q != cudaErrorNotReady) {
+                lk.lock();
+                return BLS_ERR_CUDA;
+            }
+            admitting = q == cudaSuccess;
+        }
         lk.lock();
         for (uint64_t tk : finished) done[tk] = t;
         items += finished_items;
@@ -369,6 +406,7 @@ struct bls_server {
             for (uint32_t k = 0; k < span; ++k) {
                 const uint32_t slot = (ring.pub + k) % ring.cap;
                 ring.h_res[slot] = kSentinel;
+                if (ring.split) ring.h_sub[slot] = kSentinel;
                 if (k < (uint32_t)q.n) {
                     if (ring.h_comp)
                         memcpy(ring.h_comp + 48 * (size_t)slot, q.sigs.data() + 48 * (size_t)k, 48);
@@ -393,8 +431,10 @@ struct bls_server {
         int rc = BLS_OK;
         if (ring.pub != from) {
             const uint32_t n = ring.pub - from;
-            const cudaStream_t st = ring.h_comp ? ring.dec[ring.pub_round % Ring::kDecStreams] : ring.copy;
+            const int dec_i = (int)(ring.pub_round % Ring::kDecStreams);
+            const cudaStream_t st = ring.h_comp ? ring.dec[dec_i] : ring.copy;
             if ((ring.h_comp ? (rc = ring_copy_in(ring.d_comp, ring.h_comp, 48, from, n, st)) ||
+                                   (ring.split && (rc = ring_copy_in(ring.d_sub, ring.h_sub, 1, from, n, st))) ||
                                    (rc = ring_decode(from, n, st))
                              : (rc = ring_copy_in(ring.d_sigs, ring.h_sigs, 12, from, n, st))) ||
                 (rc = ring_copy_in(ring.d_nhms, ring.h_nhms, 12, from, n, st)) ||
@@ -424,6 +464,11 @@ struct bls_server {
                 return BLS_ERR_CUDA;
             }
             ring.pub_pending.emplace_back(slot, ring.pub);
+            // split decode: the subgroup test after the publication, while the kernel verifies
+            if (ring.split && (ring_subgroup(from, n, st) || cudaEventRecord(ring.dec_idle[dec_i], st))) {
+                lk.lock();
+                return BLS_ERR_CUDA;
+            }
             progressed = true;
         }
         bool pending = false, relaunched = false;
@@ -551,7 +596,8 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
         if (cap < least) cap = least;
         cap = (cap + r.group - 1) / r.group * r.group;
         const bool comp = s->cfg.sig_format == BLS_SIG_COMPRESSED;
-        if (cap * (comp ? 252 : 200) + 64 > s->cfg.mem_cap_bytes || cap > (1u << 30)) {
+        r.split = comp && s->view.shape == bls::kShapeWide;
+        if (cap * (comp ? 256 : 200) + 64 > s->cfg.mem_cap_bytes || cap > (1u << 30)) {
             delete s;
             return BLS_ERR_NOMEM;
         }
@@ -569,6 +615,8 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
                   (!comp || (cudaHostAlloc((void**)&r.h_comp, cap * 48, 0) == cudaSuccess &&
                              cudaMalloc((void**)&r.d_comp, cap * 48) == cudaSuccess &&
                              cudaMalloc((void**)&r.d_st, cap * 4) == cudaSuccess)) &&
+                  (!r.split || (cudaHostAlloc((void**)&r.h_sub, cap * 4, 0) == cudaSuccess &&
+                                cudaMalloc((void**)&r.d_sub, cap * 4) == cudaSuccess)) &&
                   cudaStreamCreateWithFlags(&r.copy, cudaStreamNonBlocking) == cudaSuccess &&
                   cudaStreamCreateWithFlags(&r.poll, cudaStreamNonBlocking) == cudaSuccess &&
                   cudaHostAlloc((void**)&r.h_pubv, 4 * Ring::kPubSlots, 0) == cudaSuccess &&
@@ -578,7 +626,8 @@ int bls_server_create(bls_ctx* ctx, const bls_server_config* cfg, bls_server** o
         for (int k = 0; ok && k < Ring::kPubSlots; ++k)
             ok = cudaEventCreateWithFlags(&r.pub_ev[k], cudaEventDisableTiming) == cudaSuccess;
         for (int k = 0; ok && comp && k < Ring::kDecStreams; ++k)
-            ok = cudaStreamCreateWithFlags(&r.dec[k], cudaStreamNonBlocking) == cudaSuccess;
+            ok = cudaStreamCreateWithFlags(&r.dec[k], cudaStreamNonBlocking) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&r.dec_idle[k], cudaEventDisableTiming) == cudaSuccess;
         if (ok) memset(r.h_ctl, 0, 64);
         if (!ok) {
             bls_server_destroy(s);
@@ -634,15 +683,17 @@ void bls_server_destroy(bls_server* s) {
         Ring& r = s->ring;
         s->ring_stop();
         for (void* p : {(void*)r.h_sigs, (void*)r.h_nhms, (void*)r.h_ids, (void*)r.h_res, (void*)r.h_ctl,
-                        (void*)r.h_comp, (void*)r.h_pubv})
+                        (void*)r.h_comp, (void*)r.h_pubv, (void*)r.h_sub})
             if (p) cudaFreeHost(p);
         for (cudaEvent_t ev : r.pub_ev)
             if (ev) cudaEventDestroy(ev);
         if (r.poll) cudaStreamDestroy(r.poll);
         for (cudaStream_t st : r.dec)
             if (st) cudaStreamDestroy(st);
+        for (cudaEvent_t ev : r.dec_idle)
+            if (ev) cudaEventDestroy(ev);
         for (void* p : {(void*)r.d_sigs, (void*)r.d_nhms, (void*)r.d_ids, (void*)r.d_res, (void*)r.d_ctl,
-                        (void*)r.d_comp, (void*)r.d_st})
+                        (void*)r.d_comp, (void*)r.d_st, (void*)r.d_sub})
             if (p) cudaFree(p);
         if (r.done) cudaEventDestroy(r.done);
         if (r.copy) cudaStreamDestroy(r.copy);
