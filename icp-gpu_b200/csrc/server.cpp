@@ -31,7 +31,9 @@
 // its result slots holds the sentinel any more, copies its results out and
 // frees ring space in order.  Admission is by ring space.  The kernel leaves
 // when idle for 20 ms, on destroy, or 60 s after its launch; the dispatcher
-// relaunches it while work is left.
+// relaunches it while work is left.  Compressed signatures are decoded on
+// the device before their range is published, in rounds on decode streams of
+// their own (struct Ring below has the rules).
 #include <cuda_runtime.h>
 
 #include <algorithm>
