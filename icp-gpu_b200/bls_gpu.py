@@ -181,7 +181,7 @@ def batch_bls_verify(sigs, neg_hm_points, g2_prepared, pk_prepared):
     ret = lib().gpu_batch_bls_verify(_ptr(sigs), _ptr(nhms), _ptr(g2), _ptr(pk), _ptr(res), m)
     if ret != 0:
         raise GpuError("GPU kernel failed: " + last_error())
-    return [bool(r == 1) for r in res]
+    return (res == 1).tolist()
 
 
 def bls_verify(sig, neg_hm, g2_prepared, pk_prepared):
