@@ -352,14 +352,17 @@ int prepare(bls_ctx* c, size_t n, int fmt, bool want_ml, bool want_gt) {
 }
 
 // enqueue: staged inputs -> device, verify, results -> h_res (no synchronise);
-// nhms_on_device: d_nhms was filled on the device (a hash launch) instead
+// nhms_on_device: d_nhms was filled on the device (a hash launch) instead;
+// inputs_on_device: the caller has already queued every input copy
 int enqueue(bls_ctx* c, size_t n, int fmt, bool persistent, bool want_ml, bool want_gt,
-            bool nhms_on_device = false) {
+            bool nhms_on_device = false, bool inputs_on_device = false) {
     size_t sig_bytes = n * (fmt == BLS_SIG_COMPRESSED ? 48 : 96);
-    CK(cudaMemcpyAsync(c->d_sigs.p, c->h_sigs.p, sig_bytes, cudaMemcpyHostToDevice, c->stream));
-    if (!nhms_on_device)
-        CK(cudaMemcpyAsync(c->d_nhms.p, c->h_nhms.p, n * 96, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->d_pkidx.p, c->h_pkidx.p, n * 4, cudaMemcpyHostToDevice, c->stream));
+    if (!inputs_on_device) {
+        CK(cudaMemcpyAsync(c->d_sigs.p, c->h_sigs.p, sig_bytes, cudaMemcpyHostToDevice, c->stream));
+        if (!nhms_on_device)
+            CK(cudaMemcpyAsync(c->d_nhms.p, c->h_nhms.p, n * 96, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->d_pkidx.p, c->h_pkidx.p, n * 4, cudaMemcpyHostToDevice, c->stream));
+    }
     bls::VerifyArgs a{};
     a.sigs = c->d_sigs.p;
     a.sig_compressed = fmt == BLS_SIG_COMPRESSED;
@@ -748,10 +751,14 @@ int bls_verify_batch(bls_ctx* ctx, const bls_batch* b, int32_t* results) {
     size_t n = (size_t)b->n;
     size_t sig_bytes = n * (b->sig_format == BLS_SIG_COMPRESSED ? 48 : 96);
     if ((rc = prepare(ctx, n, b->sig_format, b->miller_out != nullptr, b->gt_out != nullptr))) return rc;
-    memcpy(ctx->h_sigs.p, b->sigs, sig_bytes);
-    memcpy(ctx->h_nhms.p, b->neg_hms, n * 96);
-    memcpy(ctx->h_pkidx.p, b->pk_ids, n * 4);
-    if ((rc = enqueue(ctx, n, b->sig_format, false, b->miller_out != nullptr, b->gt_out != nullptr))) return rc;
+    // the caller's buffers straight to the device (the call is synchronous, so
+    // they outlive the copies): the driver pipelines a pageable copy through
+    // its own staging, where a copy into pinned staging first would serialise
+    CK(cudaMemcpyAsync(ctx->d_sigs.p, b->sigs, sig_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_nhms.p, b->neg_hms, n * 96, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_pkidx.p, b->pk_ids, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = enqueue(ctx, n, b->sig_format, false, b->miller_out != nullptr, b->gt_out != nullptr, false, true)))
+        return rc;
     if (b->miller_out) CK(cudaMemcpyAsync(b->miller_out, ctx->d_ml.p, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
     if (b->gt_out) CK(cudaMemcpyAsync(b->gt_out, ctx->d_gt.p, n * 576, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
