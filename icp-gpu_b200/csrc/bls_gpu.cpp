@@ -801,14 +801,15 @@ int bls_verify_requests(bls_ctx* ctx, const bls_request* reqs, int nreq, int fmt
         return BLS_OK;
     }
     if ((rc = prepare(ctx, total, fmt, false, false))) return rc;
-    size_t off = 0;
-    for (int r = 0; r < nreq; ++r) {
-        size_t n = (size_t)reqs[r].n;
-        memcpy((char*)ctx->h_sigs.p + off * sb, reqs[r].sigs, n * sb);
-        memcpy((char*)ctx->h_nhms.p + off * 96, reqs[r].neg_hms, n * 96);
-        memcpy((char*)ctx->h_pkidx.p + off * 4, reqs[r].pk_ids, n * 4);
-        off += n;
-    }
+    // every request into the pinned staging at its offset, on the host's cores
+    std::vector<size_t> first((size_t)nreq + 1, 0);
+    for (int r = 0; r < nreq; ++r) first[r + 1] = first[r] + (size_t)reqs[r].n;
+    host_parallel_for(nreq, [&](int r) {
+        const size_t n = (size_t)reqs[r].n, at = first[r];
+        memcpy((char*)ctx->h_sigs.p + at * sb, reqs[r].sigs, n * sb);
+        memcpy((char*)ctx->h_nhms.p + at * 96, reqs[r].neg_hms, n * 96);
+        memcpy((char*)ctx->h_pkidx.p + at * 4, reqs[r].pk_ids, n * 4);
+    });
     std::vector<const void*> key = {(const void*)total, (const void*)(size_t)fmt,
                                     (const void*)(size_t)ctx->cfg.lanes_per_pairing,
                                     (const void*)(size_t)ctx->cfg.threads_per_block,
@@ -838,11 +839,8 @@ int bls_verify_requests(bls_ctx* ctx, const bls_request* reqs, int nreq, int fmt
     }
     CK(cudaGraphLaunch(ctx->graph, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    off = 0;
-    for (int r = 0; r < nreq; ++r) {
-        memcpy(reqs[r].results, (const char*)ctx->h_res.p + off * 4, (size_t)reqs[r].n * 4);
-        off += (size_t)reqs[r].n;
-    }
+    for (int r = 0; r < nreq; ++r)
+        memcpy(reqs[r].results, (const char*)ctx->h_res.p + first[r] * 4, (size_t)reqs[r].n * 4);
     return BLS_OK;
 }
 
@@ -1140,10 +1138,11 @@ int bls_verify_messages(bls_ctx* ctx, int fmt, const void* sigs, const uint8_t* 
     CK(cudaSetDevice(ctx->cfg.device));
     const size_t k = (size_t)n;
     if ((rc = prepare(ctx, k, fmt, false, false))) return rc;
-    memcpy(ctx->h_sigs.p, sigs, k * (fmt == BLS_SIG_COMPRESSED ? 48 : 96));
-    memcpy(ctx->h_pkidx.p, pk_ids, k * 4);
+    CK(cudaMemcpyAsync(ctx->d_sigs.p, sigs, k * (fmt == BLS_SIG_COMPRESSED ? 48 : 96), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_pkidx.p, pk_ids, k * 4, cudaMemcpyHostToDevice, ctx->stream));
     if ((rc = stage_hash(ctx, msgs, offsets, n, dst, dst_len))) return rc;
-    if ((rc = enqueue(ctx, k, fmt, false, false, false, true))) return rc;
+    if ((rc = enqueue(ctx, k, fmt, false, false, false, true, true))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     memcpy(results, ctx->h_res.p, k * 4);
     return BLS_OK;
