@@ -95,6 +95,7 @@ def lib():
         L.gpu_g1_decompress.argtypes = [P, P]
         L.gpu_msm_g1.argtypes = [P, P, ctypes.c_size_t, P]
         L.gpu_jacobian_to_affine.argtypes = [P, P]
+        L.bls_ref_cache_stats.argtypes = [P, P, P]
         L.bls_config_default.argtypes = [ctypes.POINTER(Config), I]
         L.bls_config_default.restype = None
         L.bls_ctx_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(P)]
@@ -182,6 +183,15 @@ def batch_bls_verify(sigs, neg_hm_points, g2_prepared, pk_prepared):
     if ret != 0:
         raise GpuError("GPU kernel failed: " + last_error())
     return (res == 1).tolist()
+
+
+def ref_cache_stats():
+    """The reference entry point's table cache: (resident tables, capacity,
+    times it was emptied to make room)."""
+    res, cap, fl = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_uint64(0)
+    if lib().bls_ref_cache_stats(ctypes.byref(res), ctypes.byref(cap), ctypes.byref(fl)) != 0:
+        raise GpuError("bls_ref_cache_stats failed: " + last_error())
+    return res.value, cap.value, fl.value
 
 
 def bls_verify(sig, neg_hm, g2_prepared, pk_prepared):

@@ -17,6 +17,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -106,6 +107,7 @@ struct bls_ctx {
     uint64_t* d_corr = nullptr;     // (1 + max_pks) x 12: generator, then keys
     uint8_t* d_norm_bad = nullptr;  // (1 + max_pks): a table with a zero c2
     bool norm_ok = true;            // every table normalised
+    bool g2_norm_bad = false;       // the generator's table has a zero c2
 
     // normalise table `src` into `dst`, correction factor into slot `k` of d_corr;
     // an identity key's table is never read (its pair is skipped), so a zero
@@ -116,6 +118,7 @@ struct bls_ctx {
         CK(cudaMemcpyAsync(&bad, d_norm_bad + k, 1, cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
         if (bad && !identity) norm_ok = false;
+        if (bad && k == 0) g2_norm_bad = true;
         return BLS_OK;
     }
     // normalised-line arguments of a verify over the registered tables
@@ -163,6 +166,7 @@ struct bls_ctx {
     std::unordered_multimap<uint64_t, int32_t> table_ids;
     std::vector<uint64_t> h_cached;   // table of key id k at k * 2448 (ids below n_pks)
     std::vector<uint64_t> h_g2_table; // the generator table d_g2 holds, fetched on first use
+    uint64_t cache_flushes = 0;       // times the cache was emptied to make room
 
     // Large host inputs (the reference entry point's per-item line tables,
     // 19,584 B an item) copy from pageable memory at a fraction of the link's
@@ -296,6 +300,14 @@ int default_ctx(bls_ctx** out) {
         auto* c = new bls_ctx();
         bls_config cfg;
         bls_config_default(&cfg, 0);
+        // BLS_REF_TABLE_CACHE: how many distinct key tables the reference
+        // entry point keeps on the device (default 1,024; 39 KB each with the
+        // normalised copy)
+        if (const char* e = getenv("BLS_REF_TABLE_CACHE")) {
+            const long v = strtol(e, nullptr, 10);
+            if (v < 1 || v > 65536) return fail(BLS_ERR_INVALID, "BLS_REF_TABLE_CACHE must be 1 .. 65536");
+            cfg.max_pks = (int)v;
+        }
         int rc = ctx_init(c, &cfg);
         if (rc != BLS_OK) {
             c->release();
@@ -497,7 +509,13 @@ void distinct_tables(const uint64_t* tabs, int M, std::vector<int32_t>& idx, std
 // Key ids for the distinct tables of a reference-entry call (tables[j] =
 // the caller's table of distinct table j): cached ones found by exact content,
 // new ones registered in one contiguous block and normalised in one launch.
-// False (nothing changed) when the key store has no room for the new ones.
+// When the new ones do not fit beside the cached ones, the cache is emptied
+// first and every table of this call is registered afresh (a node's key set
+// changes slowly, so the tables of earlier calls that this one does not use
+// are the ones to drop); only the tables this call uses are ever resident
+// after that.  False (nothing changed) when even this call's tables alone
+// exceed the key store.  Only the reference entry point's context registers
+// keys, so emptying the store drops nothing a caller registered.
 bool cached_table_ids(bls_ctx* c, const std::vector<const uint64_t*>& tables, std::vector<int32_t>& ids, int* rc) {
     const size_t W = bls::kCoeffU64;
     *rc = BLS_OK;
@@ -510,7 +528,17 @@ bool cached_table_ids(bls_ctx* c, const std::vector<const uint64_t*>& tables, st
         if (ids[j] < 0) fresh.push_back((int)j);
     }
     if (fresh.empty()) return true;
-    if (c->n_pks + (int)fresh.size() > c->cfg.max_pks) return false;
+    if (c->n_pks + (int)fresh.size() > c->cfg.max_pks) {
+        if ((int)tables.size() > c->cfg.max_pks) return false;
+        c->table_ids.clear();
+        c->h_cached.clear();
+        c->n_pks = 0;
+        c->norm_ok = !c->g2_norm_bad;   // no key table is left to hold a zero c2
+        c->cache_flushes++;
+        ids.assign(tables.size(), -1);
+        fresh.resize(tables.size());
+        for (size_t j = 0; j < tables.size(); ++j) fresh[j] = (int)j;
+    }
     const int first = c->n_pks;
     const size_t k = fresh.size();
     c->h_cached.resize(W * (size_t)(first + (int)k));
@@ -1251,6 +1279,16 @@ int verify_cached_speculative(bls_ctx* c, const uint64_t* sigs, const uint64_t* 
 }
 
 }  // namespace
+
+int bls_ref_cache_stats(int* resident, int* capacity, uint64_t* flushes) {
+    bls_ctx* c;
+    if (default_ctx(&c) != BLS_OK) return -1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (resident) *resident = c->n_pks;
+    if (capacity) *capacity = c->cfg.max_pks;
+    if (flushes) *flushes = c->cache_flushes;
+    return 0;
+}
 
 int gpu_crypto_init(void) {
     bls_ctx* c;

@@ -82,6 +82,17 @@ int gpu_jacobian_to_affine(const uint8_t* jacobian, uint8_t* affine);
  * reference's verify path above)
  * ==================================================================== */
 
+/* The reference entry point's table cache: gpu_batch_bls_verify keeps the
+ * distinct key line tables of earlier calls on device 0 as registered,
+ * normalised keys, found again by exact content, so repeat calls send only an
+ * item -> table index.  When a call's new tables do not fit beside the cached
+ * ones, the cache is emptied and that call's tables are registered afresh.
+ * Capacity: the environment variable BLS_REF_TABLE_CACHE when the first
+ * reference call creates the context (1 .. 65536 tables), else 1,024.
+ * resident: tables held now; capacity: the most it holds; flushes: times it
+ * was emptied.  Any pointer may be NULL.  0, or -1 without a device. */
+int bls_ref_cache_stats(int* resident, int* capacity, uint64_t* flushes);
+
 /* return codes */
 #define BLS_OK 0
 #define BLS_ERR_NODEV (-1)

@@ -76,6 +76,23 @@ def test_no_device_behaviour():
     r = np.zeros(1, dtype=np.int32)
     assert L.gpu_batch_bls_verify(z.ctypes.data, z.ctypes.data, z.ctypes.data, z.ctypes.data, r.ctypes.data, 1) == -1
     assert G.last_error() != ""
+    with pytest.raises(G.GpuError):
+        G.ref_cache_stats()
+
+
+def test_reference_cache_capacity_is_checked_before_any_device_work():
+    """A capacity outside 1 .. 65536 is refused when the reference entry
+    point's context is first created, before any device call (a fresh process,
+    since that context lives for the life of the process)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import bls_gpu as G\n"
+            "assert G.lib().bls_ref_cache_stats(None, None, None) == -1\n"
+            "assert 'BLS_REF_TABLE_CACHE' in G.last_error(), G.last_error()\n")
+    env = dict(os.environ, BLS_REF_TABLE_CACHE="0", PYTHONPATH=os.path.join(root, "icp-gpu_b200"))
+    p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
 
 
 def test_python_binding_shapes_without_gpu():
