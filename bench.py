@@ -182,16 +182,39 @@ def host_cores():
     return phys, logical
 
 
+def cpu_model():
+    """the host CPU's model name and, where the kernel reports one, its
+    highest clock (MHz)"""
+    name, mhz = None, None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and name is None:
+                    name = line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    try:
+        with open("/sys/devices/system/cpu/cpu0/cpufreq/cpuinfo_max_freq") as f:
+            mhz = round(int(f.read().strip()) / 1000.0)
+    except (OSError, ValueError):
+        pass
+    return name, mhz
+
+
 def cpu_context(rate, threads):
-    """what a reader needs to place the CPU rate: cores, threads, time per
-    verification per thread, and the reference's own single-thread figure"""
+    """what a reader needs to place the CPU rate: cores, threads, the CPU
+    model, time per verification per thread, and the reference's own
+    single-thread figure"""
     phys, logical = host_cores()
     us = 1e6 * threads / rate
+    name, mhz = cpu_model()
     return {"physical_cores": phys, "logical_cpus": logical, "threads": threads,
+            "cpu_model": name, "cpu_max_mhz": mhz,
             "us_per_verify_per_thread": round(us, 1),
             "reference_us_per_verify": REF_CPU_US_PER_VERIFY,
             "reference_us_basis": "ic_bls12_381 0.10.1 single verify on the reference authors' CPU "
-                                  "(cuda/bench_bls_verify.cu:167,228), not measured here",
+                                  "(cuda/bench_bls_verify.cu:167,228; the machine its README names, README.md:246, "
+                                  "is a Ryzen 9 9900X desktop part), not measured here",
             "rate_at_reference_speed": round(threads * 1e6 / REF_CPU_US_PER_VERIFY, 1)}
 
 
