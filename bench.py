@@ -613,6 +613,7 @@ def run_batching(G, WL, ctx, wl_headline, reps=2):
         dn = torch.from_numpy(wl["nhms"][:m].view(np.int64)).to(dev)
         di = torch.from_numpy(ids[wl["pk_index"][:m]]).to(dev)
         pts = bctx.autotune(m, ds.data_ptr(), dn.data_ptr(), di.data_ptr(), repeats=2)
+        layout_rates = bctx.limb_layout_rates()
         off = wl["offsets"]
         reqs = [(wl["sigs"][a:b], wl["nhms"][a:b], ids[wl["pk_index"][a:b]]) for a, b in zip(off[:-1], off[1:])]
         n = int(off[-1])
@@ -645,6 +646,18 @@ def run_batching(G, WL, ctx, wl_headline, reps=2):
                    for l, t, b, ms in pts],
         "chosen": {"lanes": best[0], "threads_per_block": best[1], "kernel": name(best[0], best[1]),
                    "blocks_per_sm": best[2], "ms": round(best[3], 3)}}
+    # the limb-layout dimension: product throughput of each layout in the
+    # twelve-warp kernel's setting (bls_limb_layout_rates); the verify kernels
+    # are built for the first, and the sweep shows whether it is still the fastest
+    layouts = ["12 x 32-bit limbs, limb Karatsuba, carry-chain rows (216 multiplies)",
+               "15 x 26-bit signed limbs, 225 mad.wide.s32 into 64-bit columns",
+               "14 x 28-bit limbs, 196 mad.wide.u32 into 64-bit columns"]
+    lpts = [{"layout": nm, "g_products_per_s": round(r / 1e9, 2)} for nm, r in zip(layouts, layout_rates)]
+    out["autotune"]["limb_layout_points"] = lpts
+    out["autotune"]["limb_layout_chosen"] = max(lpts, key=lambda q: q["g_products_per_s"])["layout"]
+    out["autotune"]["limb_layout_basis"] = (
+        "products/s on the whole device, one block of 384 threads per SM, operands from lane-interleaved shared "
+        "memory (bls_limb_layout_rates); every verify kernel uses the first layout")
     return out
 
 

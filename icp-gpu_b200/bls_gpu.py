@@ -117,6 +117,7 @@ def lib():
         L.bls_neg_hash_to_g1.argtypes = [P, P, P, I, P, I, P]
         L.bls_imad_chain_rate.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.bls_imad_pipe_rates.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.bls_limb_layout_rates.argtypes = [P, ctypes.POINTER(ctypes.c_double), I]
         L.bls_verify_batch_rlc.argtypes = [P, ctypes.POINTER(Batch), P, P, ctypes.POINTER(I), P]
         L.bls_verify_messages.argtypes = [P, I, P, P, P, P, I, P, I, P]
         L.bls_verify_requests.argtypes = [P, ctypes.POINTER(Request), I, I, I]
@@ -415,6 +416,14 @@ class Context:
         lo, hi = ctypes.c_double(0.0), ctypes.c_double(0.0)
         self._check(self.lib.bls_imad_pipe_rates(self.h, ctypes.byref(lo), ctypes.byref(hi)), "bls_imad_pipe_rates")
         return lo.value, hi.value
+
+    def limb_layout_rates(self):
+        """Products/s of the three limb layouts in the verify kernel's setting
+        (bls_limb_layout_rates): [12 x 32-bit Karatsuba carry chains,
+        15 x 26-bit signed wide columns, 14 x 28-bit wide columns]."""
+        v = (ctypes.c_double * 3)()
+        self._check(self.lib.bls_limb_layout_rates(self.h, v, 3), "bls_limb_layout_rates")
+        return list(v)
 
     def g1_decompress(self, compressed):
         src = np.ascontiguousarray(np.frombuffer(bytes(compressed), dtype=np.uint8))

@@ -892,6 +892,17 @@ int bls_imad_pipe_rates(bls_ctx* ctx, double* lo_per_s, double* hi_per_s) {
     return BLS_OK;
 }
 
+int bls_limb_layout_rates(bls_ctx* ctx, double* products_per_s, int n_layouts) {
+    if (!ctx || !products_per_s || n_layouts < BLS_LIMB_LAYOUTS)
+        return fail(BLS_ERR_INVALID, "need room for %d rates", BLS_LIMB_LAYOUTS);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CK(cudaSetDevice(ctx->cfg.device));
+    int rc;
+    if ((rc = ctx->grow(ctx->d_in, (size_t)ctx->sms * 384 * 4))) return rc;
+    CK(bls::measure_limb_forms(ctx->sms, 2000, (uint32_t*)ctx->d_in.p, ctx->stream, products_per_s));
+    return BLS_OK;
+}
+
 int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* points, int max_points,
                  int* n_points) {
     if (!ctx || !b || b->n <= 0) return fail(BLS_ERR_INVALID, "bad sample");

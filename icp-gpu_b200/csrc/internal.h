@@ -113,6 +113,8 @@ cudaError_t launch_verify_w_serve(const VerifyArgs& a, const uint32_t* in_status
 size_t verify_w_smem_bytes();
 int verify_w_blocks_per_sm();
 cudaError_t measure_imad_chain(int sms, int iters, uint32_t* out, cudaStream_t s, double* imad_per_s);
+// products per second of the three limb layouts (limb_forms.cu); out: sms x 384 words
+cudaError_t measure_limb_forms(int sms, int iters, uint32_t* out, cudaStream_t s, double* per_s);
 cudaError_t measure_imad_rates(int sms, int iters, uint32_t* out, cudaStream_t s, double* lo_per_s,
                                double* hi_per_s);
 size_t verify_lanes_smem_bytes(int lanes, int shape = 0);

@@ -236,6 +236,17 @@ int bls_imad_chain_rate(bls_ctx* ctx, double* imad_per_s);
  * latency covered.  Their ratio shows how far a multiprecision multiply, half
  * of whose multiplies are high words, can go toward the nominal IMAD peak. */
 int bls_imad_pipe_rates(bls_ctx* ctx, double* lo_per_s, double* hi_per_s);
+/* The autotuner's limb-layout dimension: products per second on the whole
+ * device of three layouts of a 381-bit element, each in the twelve-warp verify
+ * kernel's setting (one block of 384 threads per SM, operands loaded from
+ * lane-interleaved shared memory, every product accumulated):
+ *   [0] 12 x 32-bit limbs, limb Karatsuba with carry-chain rows into a
+ *       26-limb accumulator (the layout every verify kernel is built for),
+ *   [1] 15 x 26-bit signed limbs, 225 mad.wide.s32 into 64-bit columns,
+ *   [2] 14 x 28-bit limbs, 196 mad.wide.u32 into 64-bit columns.
+ * n_layouts must be at least BLS_LIMB_LAYOUTS. */
+#define BLS_LIMB_LAYOUTS 3
+int bls_limb_layout_rates(bls_ctx* ctx, double* products_per_s, int n_layouts);
 
 /* ---- serving: continuous batching of arriving requests ----
  * A server owns a dispatcher thread and `slots` launch slots (each a stream

@@ -157,3 +157,18 @@ def test_imad_chain_ceiling_is_plausible():
         rate = c.imad_chain_rate()
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     assert 1e12 < rate < sms * 64 * 2.1e9
+
+
+def test_limb_layout_rates_are_plausible():
+    """The autotuner's limb-layout points: each layout's product rate is
+    positive and below what the nominal IMAD peak allows for its multiply
+    count (216, 225 and 196 multiplies per product), and the 32-bit
+    carry-chain layout the verify kernels use is the fastest of the three."""
+    import torch
+    with G.Context() as c:
+        rates = c.limb_layout_rates()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert len(rates) == 3
+    for r, muls in zip(rates, (216, 225, 196)):
+        assert 1e9 < r < sms * 64 * 2.1e9 / muls
+    assert rates[0] == max(rates)
