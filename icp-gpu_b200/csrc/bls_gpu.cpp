@@ -15,10 +15,12 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -43,6 +45,85 @@ int fail(int code, const char* fmt, ...) {
     g_err = buf;
     return code;
 }
+
+// Host worker pool for the library's parallel host loops (table
+// fingerprints and comparisons of the reference entry point, request
+// staging, pinned staging of large copies).  Creating a team of threads per
+// call costs about 40 us a thread on the hosts measured, more than the work
+// of a 4,096-item fingerprint pass, so the workers are created once, on first
+// use, and wait on a condition variable between loops.  One loop runs at a
+// time (callers from other threads wait their turn); the calling thread takes
+// tasks too, so a loop finishes even with no worker (no thread could be
+// created, or the process forked after the workers started).  The pool is
+// never destroyed: its idle workers end with the process.
+class HostPool {
+  public:
+    static HostPool& get() {
+        static HostPool* p = new HostPool();
+        return *p;
+    }
+    // f(t) for t in [0, n), on the workers and the calling thread
+    void run(int n, const std::function<void(int)>& f) {
+        if (n <= 0) return;
+        std::lock_guard<std::mutex> one(run_mu_);
+        start();
+        std::unique_lock<std::mutex> lk(mu_);
+        job_ = &f;
+        tasks_ = n;
+        next_ = 0;
+        remaining_ = n;
+        cv_work_.notify_all();
+        while (next_ < tasks_) {
+            const int t = next_++;
+            lk.unlock();
+            f(t);
+            lk.lock();
+            --remaining_;
+        }
+        cv_done_.wait(lk, [&] { return remaining_ == 0; });
+        job_ = nullptr;
+        tasks_ = 0;
+    }
+    int threads() {
+        std::lock_guard<std::mutex> one(run_mu_);
+        start();
+        return (int)workers_.size() + 1;
+    }
+
+  private:
+    void start() {
+        if (started_) return;
+        started_ = true;
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int want = (int)std::min(63u, (hw ? hw : 1u) - 1u);
+        for (int i = 0; i < want; ++i) {
+            try {
+                workers_.emplace_back([this] { work(); });
+            } catch (...) {
+                break;   // fewer workers; the caller takes the rest
+            }
+        }
+        for (auto& t : workers_) t.detach();
+    }
+    void work() {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            cv_work_.wait(lk, [&] { return job_ != nullptr && next_ < tasks_; });
+            const int t = next_++;
+            const std::function<void(int)>* f = job_;
+            lk.unlock();
+            (*f)(t);
+            lk.lock();
+            if (--remaining_ == 0) cv_done_.notify_all();
+        }
+    }
+    std::mutex run_mu_, mu_;
+    std::condition_variable cv_work_, cv_done_;
+    std::vector<std::thread> workers_;
+    bool started_ = false;
+    const std::function<void(int)>* job_ = nullptr;
+    int tasks_ = 0, next_ = 0, remaining_ = 0;
+};
 
 #define CK(call)                                                                          \
     do {                                                                                  \
@@ -205,16 +286,7 @@ struct bls_ctx {
                 if (err[t] == cudaSuccess)
                     err[t] = cudaMemcpyAsync((char*)dst + off + a, stage + a, e - a, cudaMemcpyHostToDevice, stream);
             };
-            std::vector<std::thread> team;
-            for (int t = 1; t < nt; ++t) {
-                try {
-                    team.emplace_back(work, t);
-                } catch (...) {
-                    work(t);   // no thread to be had: this thread copies that share too
-                }
-            }
-            work(0);
-            for (auto& th : team) th.join();
+            HostPool::get().run(nt, work);
             for (cudaError_t e : err) CK(e);
             CK(cudaEventRecord(ev_stage[b], stream));
         }
@@ -442,24 +514,18 @@ CtxView ctx_view(bls_ctx* c) {
 
 namespace {
 
-// f(i) for i in [0, n) on up to 8 host threads
+// f(i) for i in [0, n) in up to max_threads slices on the host worker pool
 template <class F>
 void host_parallel_for(int n, F f, unsigned max_threads = 8) {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int nt = std::max(1, std::min(n, (int)std::min(max_threads, hw ? hw : 1u)));
+    const int nt = std::max(1, std::min(n, (int)std::min(max_threads, (unsigned)HostPool::get().threads())));
     auto slice = [&](int t) {
         for (int i = (int)((int64_t)n * t / nt); i < (int)((int64_t)n * (t + 1) / nt); ++i) f(i);
     };
-    std::vector<std::thread> team;
-    for (int t = 1; t < nt; ++t) {
-        try {
-            team.emplace_back(slice, t);
-        } catch (...) {
-            slice(t);   // no thread to be had: this thread takes that slice too
-        }
+    if (nt == 1) {
+        slice(0);
+        return;
     }
-    slice(0);
-    for (auto& th : team) th.join();
+    HostPool::get().run(nt, slice);
 }
 
 // a line table's fingerprint: FNV-1a over its first 12 words (candidates
