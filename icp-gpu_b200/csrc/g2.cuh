@@ -8,46 +8,86 @@
 // decoder: its callers decode keys and build their line tables on the CPU per
 // item (ic-integration/patches/ic-gpu-consensus.patch:458-461).
 //
-// Square roots in Fp2 (p = 3 mod 4) follow Algorithm 9 of Adj and
-// Rodriguez-Henriquez, "Square root computation over even extension fields"
-// (IEEE Trans. Computers, 2014): a1 = a^((p-3)/4), alpha = a1^2 a,
-// x0 = a1 a; x = u x0 when alpha = -1, else (1 + alpha)^((p-1)/2) x0.  The
-// sign is then fixed by the sort flag ("lexicographically largest": y.c1 >
-// (p-1)/2, or y.c1 = 0 and y.c0 > (p-1)/2).
+// Square roots in Fp2 = Fp[u] / (u^2 + 1) (p = 3 mod 4) by the norm method:
+// for a = a0 + a1 u with a1 != 0, x0^2 is the root d = (a0 + g) / 2 or
+// (a0 - g) / 2 of 4 d^2 - 4 a0 d - a1^2 = 0 that is a square in Fp, where
+// g^2 = a0^2 + a1^2 (the norm, a square in Fp whenever a is a square in
+// Fp2), and x1 = a1 / (2 x0); for a1 = 0 the root is sqrt(a0) or u sqrt(-a0).
+// Two exponentiations in Fp, (p + 1) / 4 for g and (p - 3) / 4 for the rest
+// (which also gives d's Legendre symbol and 1 / x0 without an inverse), where
+// Algorithm 9 of Adj and Rodriguez-Henriquez (two exponentiations in Fp2)
+// costs about 2.5 times the multiplies.  The sign is then fixed by the sort flag
+// ("lexicographically largest": y.c1 > (p-1)/2, or y.c1 = 0 and
+// y.c0 > (p-1)/2), so the decoded point does not depend on which root the
+// method finds.
 #pragma once
 #include "g1.cuh"
 #include "tower.cuh"
 
 namespace bls {
 
-// a^e for an exponent given as 6 little-endian u64 words (right to left)
-static __device__ __noinline__ fp2 fp2_pow_u64(const fp2& a, const uint64_t* e, int nbits) {
-    fp2 r = fp2_one(), base = a;
-    for (int i = 0; i < nbits; ++i) {
-        if ((e[i >> 6] >> (i & 63)) & 1) r = fp2_mul(r, base);
-        base = fp2_sqr(base);
-    }
+__device__ __forceinline__ bool fp2_eq(const fp2& a, const fp2& b) { return fp_eq(a.c0, b.c0) && fp_eq(a.c1, b.c1); }
+
+// a / 2 (a canonical; also in Montgomery form): a + p when a is odd, then one
+// right shift; a + p < 2p < 2^382, so nothing carries out of the twelve limbs
+__device__ __forceinline__ fp fp_half(const fp& a) {
+    const uint32_t m = 0u - (a.w[0] & 1u);
+    uint32_t s[12];
+    asm("add.cc.u32 %0, %12, %24;\n\t"
+        "addc.cc.u32 %1, %13, %25;\n\t"
+        "addc.cc.u32 %2, %14, %26;\n\t"
+        "addc.cc.u32 %3, %15, %27;\n\t"
+        "addc.cc.u32 %4, %16, %28;\n\t"
+        "addc.cc.u32 %5, %17, %29;\n\t"
+        "addc.cc.u32 %6, %18, %30;\n\t"
+        "addc.cc.u32 %7, %19, %31;\n\t"
+        "addc.cc.u32 %8, %20, %32;\n\t"
+        "addc.cc.u32 %9, %21, %33;\n\t"
+        "addc.cc.u32 %10, %22, %34;\n\t"
+        "addc.u32 %11, %23, %35;"
+        : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7]),
+          "=r"(s[8]), "=r"(s[9]), "=r"(s[10]), "=r"(s[11])
+        : BLS_A12(a.w), "r"(BLS_P0 & m), "r"(BLS_P1 & m), "r"(BLS_P2 & m), "r"(BLS_P3 & m), "r"(BLS_P4 & m),
+          "r"(BLS_P5 & m), "r"(BLS_P6 & m), "r"(BLS_P7 & m), "r"(BLS_P8 & m), "r"(BLS_P9 & m), "r"(BLS_P10 & m),
+          "r"(BLS_P11 & m));
+    fp r;
+#pragma unroll
+    for (int i = 0; i < 11; ++i) r.w[i] = __funnelshift_r(s[i], s[i + 1], 1);
+    r.w[11] = s[11] >> 1;
     return r;
 }
 
-__device__ __forceinline__ bool fp2_eq(const fp2& a, const fp2& b) { return fp_eq(a.c0, b.c0) && fp_eq(a.c1, b.c1); }
-
 // a square root of a (any of the two) when a is a square; *ok = false otherwise
 static __device__ __noinline__ fp2 fp2_sqrt(const fp2& a, bool* ok) {
-    const uint64_t e1[6] = {0xee7fbfffffffeaaaULL, 0x07aaffffac54ffffULL, 0xd9cc34a83dac3d89ULL,
-                            0xd91dd2e13ce144afULL, 0x92c6e9ed90d2eb35ULL, 0x0680447a8e5ff9a6ULL};  // (p-3)/4
-    const uint64_t e2[6] = {0xdcff7fffffffd555ULL, 0x0f55ffff58a9ffffULL, 0xb39869507b587b12ULL,
-                            0xb23ba5c279c2895fULL, 0x258dd3db21a5d66bULL, 0x0d0088f51cbff34dULL};  // (p-1)/2
-    fp2 a1 = fp2_pow_u64(a, e1, 379);
-    fp2 x0 = fp2_mul(a1, a);
-    fp2 alpha = fp2_mul(a1, x0);
     fp2 x;
-    const fp2 minus_one = fp2_neg(fp2_one());
-    if (fp2_eq(alpha, minus_one)) {
-        x = {fp_neg(x0.c1), x0.c0};       // u x0
+    if (fp_is_zero(a.c1)) {
+        // a in Fp: sqrt(a0) when a0 is a square, else u sqrt(-a0) (-1 is not a square)
+        const fp t = fp_sqrt_candidate(a.c0);
+        if (fp_eq(fp_sqr(t), a.c0)) x = {t, fp_zero()};
+        else x = {fp_zero(), fp_sqrt_candidate(fp_neg(a.c0))};
     } else {
-        fp2 b = fp2_pow_u64(fp2_add(fp2_one(), alpha), e2, 380);
-        x = fp2_mul(b, x0);
+        const fp n = fp_add(fp_sqr(a.c0), fp_sqr(a.c1));
+        const fp g = fp_sqrt_candidate(n);
+        if (!fp_eq(fp_sqr(g), n)) {   // the norm is not a square: neither is a
+            *ok = false;
+            return fp2_zero();
+        }
+        // d = (a0 + g) / 2 is nonzero (d (a0 - g) / 2 = -a1^2 / 4).  With
+        // t = d^((p-3)/4), d t^2 = d^((p-1)/2) is d's Legendre symbol s:
+        // s = 1: x = (d t, a1 t / 2), since (d t)^2 = d;
+        // s = -1: the other root (a0 - g) / 2 = -a1^2 / (4 d) is the square,
+        //         x = (a1 t / 2, -d t) (t^2 = -1 / d gives x0^2 - x1^2 = a0
+        //         and 2 x0 x1 = a1).
+        // No inverse and no branch on s: every lane of a warp runs the same code.
+        const uint64_t e[6] = {0xee7fbfffffffeaaaULL, 0x07aaffffac54ffffULL, 0xd9cc34a83dac3d89ULL,
+                               0xd91dd2e13ce144afULL, 0x92c6e9ed90d2eb35ULL, 0x0680447a8e5ff9a6ULL};  // (p-3)/4
+        const fp d = fp_half(fp_add(a.c0, g));
+        const fp t = fp_pow_ool(d, e, 379);
+        const fp dt = fp_mul(d, t);
+        const fp h = fp_half(fp_mul(a.c1, t));
+        const bool s_one = fp_eq(fp_mul(dt, t), fp_one());
+        const fp ndt = fp_neg(dt);
+        x = {s_one ? dt : h, s_one ? h : ndt};
     }
     *ok = fp2_eq(fp2_sqr(x), a);
     return x;

@@ -18,6 +18,7 @@ import workload_py as W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 G2_CUH = os.path.join(HERE, "..", "icp-gpu_b200", "csrc", "g2.cuh")
+G1_CUH = os.path.join(HERE, "..", "icp-gpu_b200", "csrc", "g1.cuh")
 
 
 # ------------------------------------------------------------------ CPU side
@@ -27,12 +28,18 @@ def _u64_array(text, name):
 
 
 def test_device_constants():
-    """The exponents written into the device decoder."""
-    text = open(G2_CUH).read()
-    e1, e2 = _u64_array(text, "e1"), _u64_array(text, "e2")
-    assert e1 == (B.P - 3) // 4 and e1.bit_length() == 379
-    assert e2 == (B.P - 1) // 2 and e2.bit_length() == 380
-    assert "fp2_pow_u64(a, e1, 379)" in text and "e2, 380)" in text
+    """The exponents of the device's square roots: (p + 1) / 4 in the Fp
+    square root, which the G2 decoder's Fp2 square root calls, and (p - 3) / 4
+    in the Fp2 square root itself; 379 bits each."""
+    text = open(G1_CUH).read()
+    body = text[text.index("fp_sqrt_candidate(const fp& a)"):]
+    e = _u64_array(body, "e")
+    assert e == (B.P + 1) // 4 and e.bit_length() == 379
+    assert "fp_pow_ool(a, e, 379)" in body
+    g2 = open(G2_CUH).read()
+    assert "fp_sqrt_candidate(" in g2
+    e2 = _u64_array(g2[g2.index("static __device__ __noinline__ fp2 fp2_sqrt"):], "e")
+    assert e2 == (B.P - 3) // 4 and e2.bit_length() == 379 and "fp_pow_ool(d, e, 379)" in g2
 
 
 def _psi_constants():
@@ -78,37 +85,54 @@ def test_psi_constants_and_subgroup_test():
     assert not psi_test(q) and not B.g2_in_subgroup(q)
 
 
-def sqrt_alg9(a):
-    """The device's Fp2 square root (Adj and Rodriguez-Henriquez, Algorithm 9),
-    restated: (root, ok)."""
-    a1 = B.f2_pow(a, (B.P - 3) // 4)
-    x0 = B.f2_mul(a1, a)
-    alpha = B.f2_mul(a1, x0)
-    if alpha == (B.P - 1, 0):
-        x = ((-x0[1]) % B.P, x0[0])
+def sqrt_norm(a):
+    """The device's Fp2 square root (the norm method of csrc/g2.cuh), restated
+    on integers: (root, ok, branch).  For a1 = 0: sqrt(a0) or u sqrt(-a0); else
+    g = sqrt(a0^2 + a1^2), d = (a0 + g) / 2, t = d^((p-3)/4), and x = (d t,
+    a1 t / 2) when d t^2 = 1 (d a square), else (a1 t / 2, -d t)."""
+    P = B.P
+    half = lambda v: v * pow(2, P - 2, P) % P
+    a0, a1 = a
+    if a1 == 0:
+        t = pow(a0, (P + 1) // 4, P)
+        if t * t % P == a0:
+            x, branch = (t, 0), "fp-square"
+        else:
+            x, branch = (0, pow(-a0 % P, (P + 1) // 4, P)), "fp-non-square"
     else:
-        x = B.f2_mul(B.f2_pow(B.f2_add(B.F2_ONE, alpha), (B.P - 1) // 2), x0)
-    return x, B.f2_sqr(x) == a
+        n = (a0 * a0 + a1 * a1) % P
+        g = pow(n, (P + 1) // 4, P)
+        if g * g % P != n:
+            return (0, 0), False, "norm-non-square"
+        d = half(a0 + g)
+        t = pow(d, (P - 3) // 4, P)
+        dt, h = d * t % P, half(a1 * t % P)
+        if dt * t % P == 1:
+            x, branch = (dt, h), "d-square"
+        else:
+            x, branch = (h, -dt % P), "d-non-square"
+    return x, B.f2_sqr(x) == a, branch
 
 
-def test_sqrt_algorithm9_restatement():
+def test_sqrt_norm_method_restatement():
+    """Every branch of the device's Fp2 square root, on squares and
+    non-squares: the root squares back exactly when the input is a square."""
     rng = W.SplitMix64(2024)
     cases = [(0, 0), (B.P - 1, 0), (B.P - 4, 0), (5, 0), (0, 1), (4, 4)]
     for _ in range(40):
         cases.append((rng.scalar() % B.P, rng.scalar() % B.P))
-    for _ in range(10):
+    for _ in range(20):
         t = (rng.scalar() % B.P, rng.scalar() % B.P)
         cases.append(B.f2_sqr(t))                           # squares for sure
         cases.append((rng.scalar() % B.P, 0))                # Fp elements: always squares in Fp2
-    branch_minus_one = 0
+    seen = set()
     for a in cases:
-        x, ok = sqrt_alg9(a)
+        x, ok, branch = sqrt_norm(a)
+        seen.add(branch)
         assert ok == B.f2_is_square(a), a
         if ok:
             assert B.f2_sqr(x) == a
-        a1 = B.f2_pow(a, (B.P - 3) // 4)
-        branch_minus_one += B.f2_mul(a1, B.f2_mul(a1, a)) == (B.P - 1, 0)
-    assert branch_minus_one > 0        # the alpha = -1 branch is exercised
+    assert seen == {"fp-square", "fp-non-square", "norm-non-square", "d-square", "d-non-square"}, seen
 
 
 def test_oracle_g2_round_trip_and_rejects():
