@@ -454,6 +454,8 @@ int enqueue(bls_ctx* c, size_t n, int fmt, bool persistent, bool want_ml, bool w
     a.g2 = c->d_g2;
     a.pk_tables = c->d_pk;
     c->set_norm(a);
+    a.check_keys = 1;   // ids were checked on the host; the kernel checks the copy it reads
+    a.n_keys = c->n_pks;
     a.pk_index = (const int32_t*)c->d_pkidx.p;
     a.pk_identity = c->d_pk_inf;
     a.n = (int)n;
@@ -909,7 +911,9 @@ int bls_verify_requests(bls_ctx* ctx, const bls_request* reqs, int nreq, int fmt
                                     (const void*)(size_t)ctx->cfg.threads_per_block,
                                     (const void*)(size_t)ctx->cfg.blocks_per_sm, ctx->d_sigs.p, ctx->d_nhms.p,
                                     ctx->d_pkidx.p, ctx->d_res.p, ctx->d_work.p, ctx->d_xy.p, ctx->d_st.p,
-                                    ctx->h_sigs.p, ctx->h_nhms.p, ctx->h_pkidx.p, ctx->h_res.p};
+                                    ctx->h_sigs.p, ctx->h_nhms.p, ctx->h_pkidx.p, ctx->h_res.p,
+                                    // the key count the kernel checks ids against, and the table form
+                                    (const void*)(size_t)ctx->n_pks, (const void*)(size_t)ctx->norm_ok};
     if (!ctx->graph || ctx->graph_key != key) {
         ctx->drop_graph();
         if (ctx->cfg.lanes_per_pairing > 1)   // set up outside capture
@@ -1011,6 +1015,8 @@ int bls_autotune(bls_ctx* ctx, const bls_batch* b, int repeats, bls_tune_point* 
         a.g2 = ctx->d_g2;
         a.pk_tables = ctx->d_pk;
         ctx->set_norm(a);
+        a.check_keys = 1;   // device ids: the kernel checks them
+        a.n_keys = ctx->n_pks;
         a.pk_index = b->pk_ids;
         a.pk_identity = ctx->d_pk_inf;
         a.n = b->n;
@@ -1061,6 +1067,8 @@ int bls_verify_batch_device(bls_ctx* ctx, const bls_batch* b, int32_t* results_d
     a.g2 = ctx->d_g2;
     a.pk_tables = ctx->d_pk;
     ctx->set_norm(a);
+    a.check_keys = 1;   // device ids: the kernel checks them
+    a.n_keys = ctx->n_pks;
     a.pk_index = b->pk_ids;
     a.pk_identity = ctx->d_pk_inf;
     a.n = b->n;

@@ -20,7 +20,13 @@ enum : int32_t {
     ST_X_NOT_CANONICAL = 2,
     ST_NOT_ON_CURVE = 3,
     ST_NOT_IN_SUBGROUP = 4,
+    ST_BAD_KEY_INDEX = 5,     // not a decode status: a key id outside the tables
 };
+
+// a key id the verify kernels may read (VerifyArgs::check_keys, n_keys)
+__device__ __forceinline__ bool key_index_ok(int64_t id, int check, int n_keys) {
+    return !check || (id >= 0 && id < (int64_t)n_keys);
+}
 
 __device__ __forceinline__ fp fp_four() {
     fp one = fp_one();

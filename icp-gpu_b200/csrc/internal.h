@@ -15,6 +15,11 @@ struct VerifyArgs {
     const uint64_t* g2;          // generator line table, device
     const uint64_t* pk_tables;   // k x 2448 u64, device
     const int32_t* pk_index;     // n table ids, device; NULL = table i for item i
+    // check_keys != 0: an id outside [0, n_keys) reads no table and the item's
+    // result is -BLS_ST_BAD_KEY_INDEX (a decode failure already recorded is
+    // kept); check_keys == 0: ids are not checked (the caller validated them)
+    int check_keys;
+    int n_keys;
     const uint8_t* pk_identity;  // per table, device; NULL = none is the identity
     int n;
     int32_t* results;            // n, device

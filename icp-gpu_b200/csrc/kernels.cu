@@ -43,6 +43,12 @@ __global__ void __launch_bounds__(kVerifyThreads) k_verify(VerifyArgs a) {
     fp hx = fp_load_u64(h), hy = fp_load_u64(h + 6);
     bool h_id = g1_limbs_identity(hx, hy);
     int64_t pk = a.pk_index ? (int64_t)a.pk_index[i] : (int64_t)i;
+    if (!key_index_ok(pk, a.check_keys, a.n_keys)) {   // no table read for it
+        a.results[i] = -ST_BAD_KEY_INDEX;
+        if (a.ml_out) for (int k = 0; k < 72; ++k) a.ml_out[72 * (size_t)i + k] = 0;
+        if (a.gt_out) for (int k = 0; k < 72; ++k) a.gt_out[72 * (size_t)i + k] = 0;
+        return;
+    }
     bool pk_id = a.pk_identity ? a.pk_identity[pk] != 0 : false;
     fp12 ml = miller_loop_2(sx, sy, a.g2, sig_id, hx, hy, a.pk_tables + BLS_COEFF_U64 * pk, h_id || pk_id);
     fp12 gt = final_exponentiation(ml);

@@ -488,6 +488,10 @@ __global__ void __launch_bounds__(kThreads, 6) k_verify_fp2(VerifyArgs a, const 
             fp sx = fp_load_u64_cg(s), sy = fp_load_u64_cg(s + 6);
             fp hx = fp_load_u64_cg(h), hy = fp_load_u64_cg(h + 6);
             int64_t pki = a.pk_index ? (int64_t)__ldcg(a.pk_index + item) : (int64_t)item;
+            if (!key_index_ok(pki, a.check_keys, a.n_keys)) {   // no table read for it
+                if (status == 0) status = ST_BAD_KEY_INDEX;
+                pki = 0;
+            }
             pk = (norm ? a.pk_norm : a.pk_tables) + kCoeffU64 * pki;
             if (norm) pk_cf = a.pk_corr + 12 * pki;
             skip1 = g1_limbs_identity(sx, sy) || status != 0;

@@ -242,6 +242,10 @@ __global__ void __launch_bounds__(32 * 4) k_verify_lanes(VerifyArgs a, const uin
             fp sx = fp_load_u64(s), sy = fp_load_u64(s + 6);
             fp hx = fp_load_u64(h), hy = fp_load_u64(h + 6);
             int64_t pki = a.pk_index ? (int64_t)a.pk_index[item] : (int64_t)item;
+            if (!key_index_ok(pki, a.check_keys, a.n_keys)) {   // no table read for it
+                if (status == 0) status = ST_BAD_KEY_INDEX;
+                pki = 0;
+            }
             pk = a.pk_tables + kCoeffU64 * pki;
             skip1 = g1_limbs_identity(sx, sy) || status != 0;
             skip2 = g1_limbs_identity(hx, hy) || (a.pk_identity && a.pk_identity[pki]) || status != 0;

@@ -488,6 +488,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_verify_w(VerifyArgs a, const ui
                 hx = fp_load_u64_cg(hp);
                 hy = fp_load_u64_cg(hp + 6);
                 pki = a.pk_index ? (uint32_t)__ldcg(a.pk_index + item) : item;
+                if (!key_index_ok((int64_t)(int32_t)pki, a.check_keys, a.n_keys)) {   // no table read for it
+                    if (status == 0) status = ST_BAD_KEY_INDEX;
+                    pki = 0;
+                }
                 const bool s1 = status != 0 || g1_limbs_identity(sx, sy);
                 const bool s2 = status != 0 || g1_limbs_identity(hx, hy) || (a.pk_identity && a.pk_identity[pki]);
                 skip = (s1 ? 1u : 0u) | (s2 ? 2u : 0u);

@@ -111,6 +111,8 @@ int bls_ref_cache_stats(int* resident, int* capacity, uint64_t* flushes);
 #define BLS_ST_X_NOT_CANONICAL 2   /* x >= p */
 #define BLS_ST_NOT_ON_CURVE 3      /* x^3 + 4 (G2: x^3 + 4(1 + u)) is not a square */
 #define BLS_ST_NOT_IN_SUBGROUP 4   /* on the curve, outside the order-r subgroup */
+#define BLS_ST_BAD_KEY_INDEX 5     /* not a decode status: a key id outside the tables, where the kernel
+                                      checks ids (device-resident ids, bls_verify_compressed_noalloc) */
 
 /* signature input formats */
 #define BLS_SIG_AFFINE 0      /* 12 x uint64 Montgomery x, y */
@@ -188,7 +190,10 @@ int bls_verify_batch(bls_ctx* ctx, const bls_batch* batch, int32_t* results);
 
 /* Same with every pointer in device memory (inputs already resident); the
  * call enqueues on the context stream and returns without synchronising.
- * bls_ctx_sync waits for it. */
+ * bls_ctx_sync waits for it.  The host cannot read the key ids here, so the
+ * kernel checks them: an item whose id names no registered table reads no
+ * table and gets -BLS_ST_BAD_KEY_INDEX (a compressed signature that failed to
+ * decode keeps its own status). */
 int bls_verify_batch_device(bls_ctx* ctx, const bls_batch* batch_device, int32_t* results_device);
 int bls_ctx_sync(bls_ctx* ctx);
 /* the context's CUDA stream (cudaStream_t) */
@@ -319,7 +324,6 @@ int bls_server_stats(bls_server* srv, uint64_t* launches, uint64_t* items, uint6
  * do not use this entry point across a cudaDeviceReset (the cached address
  * goes stale).  lanes_per_pairing: 2, 4, 6 or 8. */
 #define BLS_NOALLOC_MAX_ITEMS 8192
-#define BLS_ST_BAD_KEY_INDEX 5     /* bls_verify_compressed_noalloc: key index outside the caller's tables */
 int bls_verify_compressed_noalloc(const uint8_t* sigs48, const uint64_t* neg_hms, const uint64_t* g2_coeffs,
                                   const uint64_t* pk_tables, const uint8_t* pk_identity, int n_tables,
                                   const int32_t* pk_index, int32_t* results, int n, int lanes_per_pairing,
